@@ -1,0 +1,139 @@
+/* fcb200 -- B200-native fast convolution (pulse compression) for OpenVSIP.
+ *
+ * C ABI of the drop-in backend.  Plain pointers and sizes only; complex data is
+ * interleaved complex<float> (fcb_cf32), row-major, unit stride along a row,
+ * row stride in complex elements.  Every function returns FCB_OK (0) or an
+ * error code; fcb_last_error() gives the calling thread's last message.
+ *
+ * Which reference interface each entry point replaces:
+ *
+ *   fcb_plan_fftm / fcb_exec      ovxx::signal::fft::fftm_backend<complex<float>,
+ *                                 complex<float>, row, D> (src/ovxx/signal/fft/
+ *                                 backend.hpp:696-784): constructed once per
+ *                                 vsip::Fftm object with the full (rows, N) domain
+ *                                 and scale (src/ovxx/fftw/fftw.cpp:904-919), then
+ *                                 out_of_place / in_place per call with fewer or
+ *                                 equal rows (fftw.cpp:965-1001).  The scale is
+ *                                 applied inside the kernel, i.e. supports_scale()
+ *                                 is true and the workspace scale pass
+ *                                 (src/ovxx/signal/fft/workspace.hpp:474-478) is
+ *                                 skipped.
+ *   fcb_plan_fastconv / fcb_exec  the fused fast-convolution expression
+ *                                 inv_fftm(vmmul<0>(replica, fwd_fftm(data)))
+ *                                 (tests/fastconv.cpp:204; benchmarks/fastconv.cpp
+ *                                 :100-106 phased form) that the reference routes
+ *                                 through the empty be::fc_expr slot
+ *                                 (src/ovxx/dispatcher/tags.hpp:33-34) to
+ *                                 be::rbo_expr (src/ovxx/assign/rbo.hpp:18-32).
+ *                                 A replica MATRIX (one spectrum per row) covers
+ *                                 inv_fftm(W * fwd_fftm(data))
+ *                                 (tests/fastconv.cpp:213-246).
+ *   fcb_vmmul_rows                vmmul<0>(v, m) (src/vsip/impl/vmmul.hpp:114-128,
+ *                                 src/ovxx/expr/vmmul.hpp:53-59).
+ *   fcb_replica_spectrum          the replica transform t2f(weights)
+ *                                 (tests/fastconv.cpp:21-26), done in FP64 on the
+ *                                 GPU.
+ *   fcb_batch_*                   no single reference counterpart: many
+ *                                 Fftm+vmmul+Fftm jobs of uneven shapes in one
+ *                                 persistent launch.
+ *
+ * Lengths: powers of two from 1 to 65536.
+ */
+#ifndef FCB200_H
+#define FCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FCB_API __attribute__((visibility("default")))
+#else
+#define FCB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { float re, im; } fcb_cf32;
+typedef struct fcb_plan_s *fcb_plan;
+
+enum fcb_status
+{
+  FCB_OK = 0,
+  FCB_ERR_INVALID = 1,      /* bad argument (size, stride, pointer) */
+  FCB_ERR_UNSUPPORTED = 2,  /* valid request this backend does not implement */
+  FCB_ERR_CUDA = 3,         /* CUDA runtime or launch failure */
+  FCB_ERR_NOMEM = 4,        /* device or host allocation failed */
+  FCB_ERR_TIMEOUT = 5,      /* a bounded wait gave up */
+  FCB_ERR_NODEVICE = 6      /* no usable sm_100 device */
+};
+
+/* Where a buffer lives. */
+enum fcb_where { FCB_HOST = 0, FCB_DEVICE = 1 };
+
+/* Transform direction: the reference's fft_fwd (-2) / fft_inv (-1) tags map to
+ * exponents -1 / +1 (src/ovxx/signal/fft/util.hpp:41-51). */
+enum fcb_exponent { FCB_FORWARD = -1, FCB_INVERSE = +1 };
+
+/* How a replica is given. */
+enum fcb_replica_kind
+{
+  FCB_REPLICA_SPECTRUM = 0,      /* already in the frequency domain (vmmul vector) */
+  FCB_REPLICA_TIME = 1,          /* time domain: spectrum = FFT(replica), FP64 on GPU */
+  FCB_REPLICA_TIME_MATCHED = 2   /* time domain: spectrum = conj(FFT(replica)) */
+};
+
+/* Library status. */
+FCB_API const char *fcb_last_error(void);
+FCB_API const char *fcb_version(void);
+/* Select the CUDA device for subsequent plans of the calling thread. */
+FCB_API int fcb_init(int device);
+/* 1 if n is a supported row length. */
+FCB_API int fcb_supported_length(long long n);
+
+/* Row-wise multiple FFT plan: n samples per row, up to rows_max rows per call,
+ * exponent FCB_FORWARD or FCB_INVERSE, output multiplied by scale. */
+FCB_API int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale,
+                  fcb_plan *plan);
+
+/* Fused fast-convolution plan: y = IFFT(R .* FFT(x)) / n per row.
+ * replica: replica_rows rows (1 = one vector shared by all rows, or one per
+ * data row) of n samples at row stride replica_rs, kind fcb_replica_kind,
+ * located at `where`.  The plan keeps the spectrum resident on the device. */
+FCB_API int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica,
+                      long long replica_rows, long long replica_rs,
+                      int replica_kind, int where, fcb_plan *plan);
+
+/* Execute a plan on `rows` rows (rows <= rows_max).  in and out may alias
+ * (in-place).  where = FCB_DEVICE: both pointers are device pointers and the
+ * call is asynchronous on the plan's stream.  where = FCB_HOST: host pointers;
+ * the call copies through the device and returns when out is written. */
+FCB_API int fcb_exec(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out,
+             long long out_rs, long long rows, int where);
+
+/* Use a caller-owned cudaStream_t (NULL = the plan's own stream). */
+FCB_API int fcb_set_stream(fcb_plan plan, void *stream);
+/* Wait for all work queued on the plan's stream. */
+FCB_API int fcb_sync(fcb_plan plan);
+FCB_API int fcb_destroy(fcb_plan plan);
+
+/* Plan introspection: the kernel configuration chosen for this plan. */
+FCB_API int fcb_plan_info(fcb_plan plan, long long *n, int *cluster_ctas,
+                  int *rows_per_cta, int *smem_bytes);
+
+/* out[r][c] = v[c] * m[r][c] on the device (asynchronous on `stream`). */
+FCB_API int fcb_vmmul_rows(const fcb_cf32 *v, const fcb_cf32 *m, long long m_rs,
+                   fcb_cf32 *out, long long out_rs, long long rows,
+                   long long cols, void *stream);
+
+/* Replica spectrum in FP64 on the GPU, rounded to complex<float>:
+ * spectrum = FFT(replica) or conj(FFT(replica)) (matched), n a power of two.
+ * Device pointers; synchronous. */
+FCB_API int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int matched,
+                         fcb_cf32 *spectrum_dev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

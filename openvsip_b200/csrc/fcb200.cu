@@ -1,0 +1,297 @@
+// C-ABI implementation of the fcb200 backend: plans, FP64 table builders,
+// kernel dispatch and host-buffer staging.  Entry points are declared in
+// include/fcb200.h, which also cites the reference interface each replaces.
+#include "fcb200.h"
+#include "fcb_engine.cuh"
+#include "fcb_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+
+namespace fcb {
+
+// ---------------------------------------------------------------------------
+// Error reporting: thread-local message, status code returned to the caller.
+static thread_local char g_err[512] = "";
+
+int set_error(int code, const char *fmt, ...)
+{
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+const char *error_text() { return g_err; }
+
+int cuda_error(cudaError_t e, const char *what)
+{
+  return set_error(FCB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// Runtime view of the compile-time schedule (for table builders).
+SchedRT sched_rt(int logn)
+{
+  SchedRT s;
+  s.logn = logn;
+  s.n = 1 << logn;
+  s.ns = (logn <= 5) ? 1 : 1 + (logn - 5 + 3) / 4;
+  s.r1 = 1 << (logn - 4 * (s.ns - 1));
+  s.d = s.n / s.r1;
+  s.half = s.n / 2;
+  int off = s.half;
+  s.tw_size = off;
+  for (int k = 2; k <= s.ns; ++k) s.tw_size += s.d >> (4 * (k - 2));
+  return s;
+}
+
+// Twiddle tables in FP64, rounded to float (forward sign; kernels conjugate).
+//   stage 1:   [q'*D + n]          = (W^{n 2q'}.re, W^{n(2q'+1)}.re, W^{n 2q'}.im, W^{n(2q'+1)}.im), W = e^{-2 pi i/N}
+//   stage s:   [off_s + q*S_s + n] = (w.re, w.re, w.im, w.im),  w = e^{-2 pi i n q / L_s}
+__global__ void build_tw_kernel(float4 *tw, SchedRT s)
+{
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= s.tw_size) return;
+  if (i < s.half)
+  {
+    long long qp = i / s.d, n = i % s.d;
+    long long m0 = (n * (2 * qp)) % s.n, m1 = (n * (2 * qp + 1)) % s.n;
+    double s0, c0, s1, c1;
+    sincospi(-2.0 * (double)m0 / (double)s.n, &s0, &c0);
+    sincospi(-2.0 * (double)m1 / (double)s.n, &s1, &c1);
+    tw[i] = make_float4((float)c0, (float)c1, (float)s0, (float)s1);
+    return;
+  }
+  long long off = s.half;
+  for (int k = 2; k <= s.ns; ++k)
+  {
+    long long L = s.d >> (4 * (k - 2)), St = L / 16;
+    if (i < off + L)
+    {
+      long long j = i - off, q = j / St, n = j % St;
+      long long m = (n * q) % L;
+      double sn, cs;
+      sincospi(-2.0 * (double)m / (double)L, &sn, &cs);
+      tw[i] = make_float4((float)cs, (float)cs, (float)sn, (float)sn);
+      return;
+    }
+    off += L;
+  }
+}
+
+// Replica pair table in slot order: slot sigma = q'*D + P holds
+// (R[k]/N, R[k+1]/N) split, k = 2q' + R1 * digitrev16(P).  1/N is exact.
+__global__ void build_rep_kernel(const float2 *spec, long long spec_rs, float4 *rep,
+                                 long long rows, SchedRT s)
+{
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long total = rows * s.half;
+  if (i >= total) return;
+  long long r = i / s.half, sigma = i % s.half;
+  int qp = (int)(sigma / s.d), P = (int)(sigma % s.d);
+  int k = 2 * qp + s.r1 * digitrev16(P, s.ns - 1);
+  const float inv = 1.0f / (float)s.n;
+  float2 a = spec[r * spec_rs + k], b = spec[r * spec_rs + k + 1];
+  rep[i] = make_float4(a.x * inv, b.x * inv, a.y * inv, b.y * inv);
+}
+
+// FP64 radix-2 Stockham FFT of one vector in global memory, one CTA.
+// Used once per replica (plan time), so simplicity beats speed here.
+__global__ void fft_fp64_kernel(const float2 *in, double2 *buf0, double2 *buf1, long long n,
+                                int matched, float2 *out)
+{
+  for (long long i = threadIdx.x; i < n; i += blockDim.x)
+    buf0[i] = make_double2(in[i].x, in[i].y);
+  __syncthreads();
+  double2 *src = buf0, *dst = buf1;
+  // Stockham autosort, radix 2: for each pass with sub-length l (1, 2, 4, ...)
+  for (long long l = 1; l < n; l <<= 1)
+  {
+    long long half = n / 2;
+    for (long long j = threadIdx.x; j < half; j += blockDim.x)
+    {
+      long long k = j % l;                  // index within the current sub-transform
+      long long base = (j / l) * 2 * l;     // output block
+      double2 a = src[j], b = src[j + half];
+      double sn, cs;
+      sincospi(-(double)k / (double)l, &sn, &cs);  // e^{-i pi k / l}
+      double2 tb = make_double2(b.x * cs - b.y * sn, b.x * sn + b.y * cs);
+      dst[base + k] = make_double2(a.x + tb.x, a.y + tb.y);
+      dst[base + k + l] = make_double2(a.x - tb.x, a.y - tb.y);
+    }
+    __syncthreads();
+    double2 *tmp = src; src = dst; dst = tmp;
+  }
+  for (long long i = threadIdx.x; i < n; i += blockDim.x)
+    out[i] = make_float2((float)src[i].x, (float)(matched ? -src[i].y : src[i].y));
+}
+
+__global__ void vmmul_kernel(const float2 *v, const float2 *m, long long m_rs, float2 *out,
+                             long long out_rs, long long rows, long long cols)
+{
+  long long total = rows * cols;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x)
+  {
+    long long r = i / cols, c = i % cols;
+    float2 a = v[c], b = m[r * m_rs + c];
+    out[r * out_rs + c] = make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  }
+}
+
+// Length-1 rows: out = in * w (w = scale, or the replica value).
+__global__ void scale_rows_kernel(const float2 *in, long long in_rs, float2 *out, long long out_rs,
+                                  long long rows, const float4 *rep, long long rep_rs, float scale)
+{
+  long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= rows) return;
+  float2 x = in[r * in_rs];
+  if (rep)
+  {
+    float4 w = rep[r * rep_rs];  // (re, -, im, -) of the single-sample spectrum / 1
+    out[r * out_rs] = make_float2(x.x * w.x - x.y * w.z, x.x * w.z + x.y * w.x);
+  }
+  else
+    out[r * out_rs] = make_float2(x.x * scale, x.y * scale);
+}
+
+// ---------------------------------------------------------------------------
+// Kernel table.
+template <int LOGN, int MODE>
+static KernelInfo make_info()
+{
+  using S = Sched<LOGN>;
+  KernelInfo k;
+  k.fn = (const void *)&rows_kernel<LOGN, MODE>;
+  k.cluster = S::CS;
+  k.rows_per_cta = S::ROWS;
+  k.smem = S::SLOTS * 16;
+  k.tw_size = S::tw_size();
+  return k;
+}
+
+template <int LOGN>
+static void fill_table(KernelInfo (*tab)[3])
+{
+  if constexpr (LOGN >= 1)
+  {
+    tab[LOGN][kFwd] = make_info<LOGN, kFwd>();
+    tab[LOGN][kInv] = make_info<LOGN, kInv>();
+    tab[LOGN][kFastconv] = make_info<LOGN, kFastconv>();
+    fill_table<LOGN - 1>(tab);
+  }
+}
+
+static KernelInfo g_table[kMaxLogN + 1][3];
+static std::once_flag g_table_once;
+
+const KernelInfo *kernel_info(int logn, int mode)
+{
+  std::call_once(g_table_once, [] { fill_table<kMaxLogN>(g_table); });
+  if (logn < 1 || logn > kMaxLogN) return nullptr;
+  return &g_table[logn][mode];
+}
+
+int prepare_kernel(const KernelInfo *k)
+{
+  // Idempotent; cheap after the first call per device.
+  cudaError_t e = cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem);
+  if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(smem)");
+  return FCB_OK;
+}
+
+int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaStream_t st)
+{
+  if (rows <= 0) return FCB_OK;
+  long long ctas = k->cluster > 1 ? rows * k->cluster : (rows + k->rows_per_cta - 1) / k->rows_per_cta;
+  if (ctas > 0x7fffffffLL) return set_error(FCB_ERR_INVALID, "too many rows in one call");
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ctas);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = k->smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  if (k->cluster > 1)
+  {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = k->cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  void *params[] = {const_cast<RowArgs *>(&args)};
+  cudaError_t e = cudaLaunchKernelExC(&cfg, k->fn, params);
+  if (e != cudaSuccess) return cuda_error(e, "row kernel launch");
+  return FCB_OK;
+}
+
+int build_twiddles(int logn, float4 **out, cudaStream_t st)
+{
+  SchedRT s = sched_rt(logn);
+  float4 *tw = nullptr;
+  cudaError_t e = cudaMalloc(&tw, sizeof(float4) * (size_t)s.tw_size);
+  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "twiddle table: %s", cudaGetErrorString(e));
+  build_tw_kernel<<<(unsigned)((s.tw_size + 255) / 256), 256, 0, st>>>(tw, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { cudaFree(tw); return cuda_error(e, "twiddle build"); }
+  *out = tw;
+  return FCB_OK;
+}
+
+int build_replica_table(int logn, const float2 *spec_dev, long long spec_rs, long long rows,
+                        float4 *rep_dev, cudaStream_t st)
+{
+  SchedRT s = sched_rt(logn);
+  long long total = rows * s.half;
+  build_rep_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(spec_dev, spec_rs, rep_dev, rows, s);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "replica table build");
+  return FCB_OK;
+}
+
+int replica_spectrum_dev(const float2 *rep_dev, long long n, int matched, float2 *spec_dev,
+                         cudaStream_t st)
+{
+  double2 *buf = nullptr;
+  cudaError_t e = cudaMallocAsync(&buf, sizeof(double2) * 2 * (size_t)n, st);
+  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "replica FFT buffer: %s", cudaGetErrorString(e));
+  fft_fp64_kernel<<<1, 1024, 0, st>>>(rep_dev, buf, buf + n, n, matched, spec_dev);
+  e = cudaGetLastError();
+  cudaFreeAsync(buf, st);
+  if (e != cudaSuccess) return cuda_error(e, "replica FFT");
+  return FCB_OK;
+}
+
+int launch_vmmul(const float2 *v, const float2 *m, long long m_rs, float2 *out, long long out_rs,
+                 long long rows, long long cols, cudaStream_t st)
+{
+  long long total = rows * cols;
+  if (total <= 0) return FCB_OK;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  vmmul_kernel<<<(unsigned)blocks, 256, 0, st>>>(v, m, m_rs, out, out_rs, rows, cols);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "vmmul launch");
+  return FCB_OK;
+}
+
+int launch_scale_rows(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
+                      const float4 *rep, long long rep_rs, float scale, cudaStream_t st)
+{
+  if (rows <= 0) return FCB_OK;
+  scale_rows_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(in, in_rs, out, out_rs, rows, rep,
+                                                                    rep_rs, scale);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "scale launch");
+  return FCB_OK;
+}
+
+}  // namespace fcb

@@ -1,0 +1,395 @@
+// fcb200 C ABI: plan objects and execution (declarations in include/fcb200.h).
+#include "fcb200.h"
+#include "fcb_engine.cuh"
+#include "fcb_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+
+using namespace fcb;
+
+struct fcb_plan_s
+{
+  int device = 0;
+  long long n = 0;
+  int logn = 0;
+  int mode = kFwd;
+  long long rows_max = 0;
+  float scale = 1.f;
+  const KernelInfo *k = nullptr;
+  float4 *tw = nullptr;
+  float4 *rep = nullptr;          // fastconv: replica pair table(s), slot order
+  long long rep_rows = 0;         // 1 = shared vector, else one per data row
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;  // current stream (own or caller's)
+  cudaStream_t aux = nullptr;     // second stream for host pipelining
+  float2 *stage[2] = {nullptr, nullptr};
+  long long stage_rows = 0;
+  cudaEvent_t done[2] = {nullptr, nullptr};
+};
+
+namespace {
+
+int log2_exact(long long n)
+{
+  if (n < 1 || (n & (n - 1)) != 0) return -1;
+  int l = 0;
+  while ((1LL << l) < n) ++l;
+  return l;
+}
+
+struct DeviceGuard
+{
+  int prev = -1;
+  explicit DeviceGuard(int dev)
+  {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard()
+  {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int check_device()
+{
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return set_error(FCB_ERR_NODEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceProp p;
+  e = cudaGetDeviceProperties(&p, dev);
+  if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceProperties");
+  if (p.major < 10) return set_error(FCB_ERR_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a", dev, p.major, p.minor);
+  return FCB_OK;
+}
+
+void plan_free(fcb_plan p)
+{
+  if (!p) return;
+  DeviceGuard g(p->device);
+  if (p->own_stream) cudaStreamSynchronize(p->own_stream);
+  if (p->aux) cudaStreamSynchronize(p->aux);
+  cudaFree(p->tw);
+  cudaFree(p->rep);
+  cudaFree(p->stage[0]);
+  cudaFree(p->stage[1]);
+  for (auto &e : p->done) if (e) cudaEventDestroy(e);
+  if (p->own_stream) cudaStreamDestroy(p->own_stream);
+  if (p->aux) cudaStreamDestroy(p->aux);
+  delete p;
+}
+
+int plan_common(fcb_plan p, long long n, long long rows_max, int mode)
+{
+  int rc = check_device();
+  if (rc) return rc;
+  cudaGetDevice(&p->device);
+  p->n = n;
+  p->logn = log2_exact(n);
+  p->mode = mode;
+  p->rows_max = rows_max;
+  cudaError_t e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_error(e, "cudaStreamCreate");
+  p->stream = p->own_stream;
+  if (p->logn >= 1)
+  {
+    p->k = kernel_info(p->logn, mode);
+    rc = prepare_kernel(p->k);
+    if (rc) return rc;
+    rc = build_twiddles(p->logn, &p->tw, p->stream);
+    if (rc) return rc;
+  }
+  return FCB_OK;
+}
+
+// Device-pointer execution on stream st.
+int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
+                long long rows, long long row0, cudaStream_t st)
+{
+  const float4 *rep = p->rep ? p->rep + (p->rep_rows > 1 ? row0 * (p->n > 1 ? p->n / 2 : 1) : 0) : nullptr;
+  long long rep_rs = p->rep_rows > 1 ? (p->n > 1 ? p->n / 2 : 1) : 0;
+  if (p->logn == 0)
+    return launch_scale_rows(in, in_rs, out, out_rs, rows, p->mode == kFastconv ? rep : nullptr, rep_rs,
+                             p->scale, st);
+  RowArgs a;
+  a.in = in;
+  a.in_rs = in_rs;
+  a.out = out;
+  a.out_rs = out_rs;
+  a.rows = rows;
+  a.tw = p->tw;
+  a.rep = rep;
+  a.rep_rs = rep_rs;
+  a.scale = p->scale;
+  return launch_rows(p->k, rows, a, st);
+}
+
+int ensure_staging(fcb_plan p, long long chunk_rows)
+{
+  if (p->stage_rows >= chunk_rows) return FCB_OK;
+  cudaFree(p->stage[0]);
+  cudaFree(p->stage[1]);
+  p->stage[0] = p->stage[1] = nullptr;
+  p->stage_rows = 0;
+  for (int i = 0; i < 2; ++i)
+  {
+    cudaError_t e = cudaMalloc(&p->stage[i], sizeof(float2) * (size_t)(chunk_rows * p->n));
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "staging buffer: %s", cudaGetErrorString(e));
+  }
+  if (!p->aux)
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_error(e, "cudaStreamCreate");
+    for (auto &ev : p->done)
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+        return cuda_error(e, "cudaEventCreate");
+  }
+  p->stage_rows = chunk_rows;
+  return FCB_OK;
+}
+
+// Host-pointer execution: rows move through two device staging buffers in
+// chunks on two streams, so one chunk's copies overlap the other's kernel.
+int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
+              long long rows)
+{
+  const size_t row_bytes = sizeof(float2) * (size_t)p->n;
+  long long chunk = std::max<long long>(1, (16LL << 20) / (long long)row_bytes);
+  if (p->k && p->k->cluster == 1) chunk = std::max<long long>(chunk, p->k->rows_per_cta);
+  chunk = std::min(chunk, rows);
+  int rc = ensure_staging(p, chunk);
+  if (rc) return rc;
+  cudaStream_t st[2] = {p->stream, p->aux};
+  // the aux stream must not start before earlier work on the plan stream
+  cudaEventRecord(p->done[1], p->stream);
+  cudaStreamWaitEvent(p->aux, p->done[1], 0);
+  int i = 0;
+  for (long long r0 = 0; r0 < rows; r0 += chunk, i ^= 1)
+  {
+    long long nr = std::min(chunk, rows - r0);
+    float2 *buf = p->stage[i];
+    cudaError_t e = cudaMemcpy2DAsync(buf, row_bytes, in + r0 * in_rs, sizeof(float2) * (size_t)in_rs,
+                                      row_bytes, (size_t)nr, cudaMemcpyHostToDevice, st[i]);
+    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, st[i]);
+    if (rc) return rc;
+    e = cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,
+                          (size_t)nr, cudaMemcpyDeviceToHost, st[i]);
+    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+  }
+  cudaError_t e1 = cudaStreamSynchronize(st[0]);
+  cudaError_t e2 = cudaStreamSynchronize(st[1]);
+  if (e1 != cudaSuccess) return cuda_error(e1, "fcb_exec (host)");
+  if (e2 != cudaSuccess) return cuda_error(e2, "fcb_exec (host)");
+  return FCB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fcb_last_error(void)
+{
+  return error_text();
+}
+
+const char *fcb_version(void) { return "fcb200 0.1 (sm_100a)"; }
+
+int fcb_init(int device)
+{
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) return set_error(FCB_ERR_NODEVICE, "no CUDA device");
+  if (device < 0 || device >= count) return set_error(FCB_ERR_INVALID, "device %d out of range [0,%d)", device, count);
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_error(e, "cudaSetDevice");
+  return check_device();
+}
+
+int fcb_supported_length(long long n)
+{
+  int l = log2_exact(n);
+  return l >= 0 && l <= kMaxLogN;
+}
+
+int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale, fcb_plan *plan)
+{
+  if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
+  *plan = nullptr;
+  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "row length %lld is not a power of two in [1, 65536]", n);
+  if (rows_max < 0) return set_error(FCB_ERR_INVALID, "rows_max < 0");
+  if (exponent != FCB_FORWARD && exponent != FCB_INVERSE) return set_error(FCB_ERR_INVALID, "exponent must be -1 or +1");
+  fcb_plan p = new (std::nothrow) fcb_plan_s;
+  if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
+  p->scale = scale;
+  int rc = plan_common(p, n, rows_max, exponent == FCB_FORWARD ? kFwd : kInv);
+  if (!rc)
+  {
+    cudaError_t e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) rc = cuda_error(e, "plan tables");
+  }
+  if (rc) { plan_free(p); return rc; }
+  *plan = p;
+  return FCB_OK;
+}
+
+int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long long replica_rows,
+                      long long replica_rs, int replica_kind, int where, fcb_plan *plan)
+{
+  if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
+  *plan = nullptr;
+  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "row length %lld is not a power of two in [1, 65536]", n);
+  if (!replica) return set_error(FCB_ERR_INVALID, "replica is NULL");
+  if (replica_rows < 1) return set_error(FCB_ERR_INVALID, "replica_rows < 1");
+  if (replica_rows > 1 && replica_rs < n) return set_error(FCB_ERR_INVALID, "replica row stride < n");
+  if (replica_kind < FCB_REPLICA_SPECTRUM || replica_kind > FCB_REPLICA_TIME_MATCHED)
+    return set_error(FCB_ERR_INVALID, "bad replica kind");
+  if (where != FCB_HOST && where != FCB_DEVICE) return set_error(FCB_ERR_INVALID, "bad location");
+  fcb_plan p = new (std::nothrow) fcb_plan_s;
+  if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
+  int rc = plan_common(p, n, rows_max, kFastconv);
+  float2 *spec = nullptr, *tmp = nullptr;
+  if (!rc)
+  {
+    const long long rs = replica_rows > 1 ? replica_rs : n;
+    const size_t bytes = sizeof(float2) * (size_t)(replica_rows * n);
+    cudaError_t e = cudaMalloc(&spec, bytes);
+    if (e != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "replica buffer: %s", cudaGetErrorString(e));
+    if (!rc)
+    {
+      e = cudaMemcpy2DAsync(spec, sizeof(float2) * (size_t)n, replica, sizeof(float2) * (size_t)rs,
+                            sizeof(float2) * (size_t)n, (size_t)replica_rows,
+                            where == FCB_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, p->stream);
+      if (e != cudaSuccess) rc = cuda_error(e, "replica copy");
+    }
+    if (!rc && replica_kind != FCB_REPLICA_SPECTRUM)
+    {
+      e = cudaMalloc(&tmp, bytes);
+      if (e != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "replica buffer: %s", cudaGetErrorString(e));
+      for (long long r = 0; !rc && r < replica_rows; ++r)
+        rc = replica_spectrum_dev(spec + r * n, n, replica_kind == FCB_REPLICA_TIME_MATCHED, tmp + r * n, p->stream);
+      if (!rc) std::swap(spec, tmp);
+    }
+    if (!rc)
+    {
+      const long long slots = n > 1 ? n / 2 : 1;
+      e = cudaMalloc(&p->rep, sizeof(float4) * (size_t)(replica_rows * slots));
+      if (e != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "replica table: %s", cudaGetErrorString(e));
+      p->rep_rows = replica_rows;
+      if (!rc)
+      {
+        if (p->logn >= 1)
+          rc = build_replica_table(p->logn, spec, n, replica_rows, p->rep, p->stream);
+        else
+        {
+          // length 1: table entry (R.re, -, R.im, -)
+          cudaMemset2DAsync(p->rep, sizeof(float4), 0, sizeof(float4), (size_t)replica_rows, p->stream);
+          e = cudaMemcpy2DAsync(p->rep, sizeof(float4), spec, sizeof(float2), sizeof(float), (size_t)replica_rows,
+                                cudaMemcpyDeviceToDevice, p->stream);
+          if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(reinterpret_cast<char *>(p->rep) + 8, sizeof(float4),
+                                  reinterpret_cast<char *>(spec) + 4, sizeof(float2), sizeof(float),
+                                  (size_t)replica_rows, cudaMemcpyDeviceToDevice, p->stream);
+          if (e != cudaSuccess) rc = cuda_error(e, "replica table (n=1)");
+        }
+      }
+    }
+    if (!rc)
+    {
+      e = cudaStreamSynchronize(p->stream);
+      if (e != cudaSuccess) rc = cuda_error(e, "replica preparation");
+    }
+  }
+  cudaFree(spec);
+  cudaFree(tmp);
+  if (rc) { plan_free(p); return rc; }
+  *plan = p;
+  return FCB_OK;
+}
+
+int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, long long out_rs,
+             long long rows, int where)
+{
+  if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
+  if (rows < 0 || rows > p->rows_max) return set_error(FCB_ERR_INVALID, "rows %lld outside [0, %lld]", rows, p->rows_max);
+  if (p->mode == kFastconv && p->rep_rows > 1 && rows > p->rep_rows)
+    return set_error(FCB_ERR_INVALID, "rows %lld exceed the replica matrix rows %lld", rows, p->rep_rows);
+  if (rows == 0) return FCB_OK;
+  if (!in || !out) return set_error(FCB_ERR_INVALID, "NULL data pointer");
+  if (in_rs < p->n || out_rs < p->n) return set_error(FCB_ERR_INVALID, "row stride smaller than the row length");
+  if (where != FCB_HOST && where != FCB_DEVICE) return set_error(FCB_ERR_INVALID, "bad location");
+  // in-place with different strides would overlap rows
+  if ((const void *)in == (const void *)out && in_rs != out_rs)
+    return set_error(FCB_ERR_INVALID, "in-place call with different row strides");
+  DeviceGuard g(p->device);
+  const float2 *i2 = reinterpret_cast<const float2 *>(in);
+  float2 *o2 = reinterpret_cast<float2 *>(out);
+  if (where == FCB_DEVICE) return exec_device(p, i2, in_rs, o2, out_rs, rows, 0, p->stream);
+  return exec_host(p, i2, in_rs, o2, out_rs, rows);
+}
+
+int fcb_set_stream(fcb_plan p, void *stream)
+{
+  if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
+  p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+  return FCB_OK;
+}
+
+int fcb_sync(fcb_plan p)
+{
+  if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
+  DeviceGuard g(p->device);
+  cudaError_t e = cudaStreamSynchronize(p->stream);
+  if (e != cudaSuccess) return cuda_error(e, "fcb_sync");
+  return FCB_OK;
+}
+
+int fcb_destroy(fcb_plan p)
+{
+  plan_free(p);
+  return FCB_OK;
+}
+
+int fcb_plan_info(fcb_plan p, long long *n, int *cluster_ctas, int *rows_per_cta, int *smem_bytes)
+{
+  if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
+  if (n) *n = p->n;
+  if (cluster_ctas) *cluster_ctas = p->k ? p->k->cluster : 1;
+  if (rows_per_cta) *rows_per_cta = p->k ? p->k->rows_per_cta : 1;
+  if (smem_bytes) *smem_bytes = p->k ? p->k->smem : 0;
+  return FCB_OK;
+}
+
+int fcb_vmmul_rows(const fcb_cf32 *v, const fcb_cf32 *m, long long m_rs, fcb_cf32 *out, long long out_rs,
+                   long long rows, long long cols, void *stream)
+{
+  if (rows < 0 || cols < 0) return set_error(FCB_ERR_INVALID, "negative size");
+  if (rows == 0 || cols == 0) return FCB_OK;
+  if (!v || !m || !out) return set_error(FCB_ERR_INVALID, "NULL pointer");
+  if (m_rs < cols || out_rs < cols) return set_error(FCB_ERR_INVALID, "row stride smaller than cols");
+  return launch_vmmul(reinterpret_cast<const float2 *>(v), reinterpret_cast<const float2 *>(m), m_rs,
+                      reinterpret_cast<float2 *>(out), out_rs, rows, cols, (cudaStream_t)stream);
+}
+
+int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int matched, fcb_cf32 *spectrum_dev)
+{
+  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "length %lld is not a power of two in [1, 65536]", n);
+  if (!replica_dev || !spectrum_dev) return set_error(FCB_ERR_INVALID, "NULL pointer");
+  int rc = check_device();
+  if (rc) return rc;
+  rc = replica_spectrum_dev(reinterpret_cast<const float2 *>(replica_dev), n, matched,
+                            reinterpret_cast<float2 *>(spectrum_dev), 0);
+  if (rc) return rc;
+  cudaError_t e = cudaStreamSynchronize(0);
+  if (e != cudaSuccess) return cuda_error(e, "replica spectrum");
+  return FCB_OK;
+}
+
+}  // extern "C"

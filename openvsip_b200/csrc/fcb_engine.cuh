@@ -1,0 +1,552 @@
+// Device engine for row-wise power-of-two FFTs and the fused fast convolution
+// (forward row FFT -> multiply by replica spectrum -> inverse row FFT * 1/N).
+//
+// Reference behaviour replaced (the reference's CPU path):
+//   forward / inverse Fftm      src/ovxx/fftw/fftw.cpp:965-977 (row loop of
+//                               fftwf_execute_dft), scale pass in
+//                               src/ovxx/signal/fft/workspace.hpp:474-478
+//   vmmul<0>                    src/ovxx/expr/vmmul.hpp:53-59
+//   fused fast convolution      benchmarks/fastconv.cpp:100-106 (phased) and
+//                               tests/fastconv.cpp:204 (by-value expression)
+//
+// Algorithm (decimation in frequency, "complex pairs"):
+//  * A thread owns 32 complex samples held as 16 complex PAIRS in split form
+//    {re: (a.re, b.re), im: (a.im, b.im)} so that every butterfly, twiddle and
+//    replica multiply runs on Blackwell's packed f32x2 add/mul/fma, two complex
+//    lanes per instruction.
+//  * Stage 1 is a radix-R1 DIF step over the whole row (stride N/R1).  Its first
+//    radix-2 level is done in scalar and places the even-q outputs in lane 0 and
+//    the odd-q outputs in lane 1, so every later operation is lane-parallel with
+//    identical constants in both lanes.  Sub-problem 2q' and 2q'+1 (length
+//    D = N/R1 each) then live side by side in one "slot" (16 bytes).
+//  * Stages 2.. are radix-16 DIF steps inside the sub-problem pairs, in place
+//    in a 16-byte-slot shared-memory array (XOR swizzle against bank conflicts).
+//    A thread reads and writes only its own group's slots inside a stage, so
+//    one barrier per exchange suffices.
+//  * After the last forward stage a slot sigma = q'*D + P holds X[k], X[k+1]
+//    with k = 2q' + R1 * digitrev16(P).  The fused path multiplies by a replica
+//    table stored in that order (scaled by 1/N, exact for powers of two) and
+//    runs the exact transpose of the forward stages with conjugate twiddles, so
+//    no reordering pass is ever needed and every row makes one HBM read and one
+//    HBM write.  The standalone FFTs add one reorder exchange.
+//  * Rows of N <= 8192 samples: one CTA of 256 threads holds 8192 samples
+//    (8192/N rows).  N >= 16384: a thread-block cluster of N/8192 CTAs holds one
+//    row; the two exchanges adjacent to stage 1 cross CTAs through distributed
+//    shared memory (stores forward, loads inverse).  No TMA multicast is used.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cooperative_groups.h>
+#include <stdint.h>
+#include <type_traits>
+
+namespace fcb {
+
+namespace cg = cooperative_groups;
+
+constexpr int kThreads = 256;        // threads per CTA
+constexpr int kSlotsPerCta = 4096;   // 16-byte slots (complex pairs) per CTA
+constexpr int kMaxLogN = 16;
+
+// ---------------------------------------------------------------------------
+// Schedule of a length-2^LOGN row transform.
+template <int LOGN>
+struct Sched
+{
+  static constexpr int N = 1 << LOGN;
+  static constexpr int NS = (LOGN <= 5) ? 1 : 1 + (LOGN - 5 + 3) / 4;  // stages
+  static constexpr int LOGR1 = LOGN - 4 * (NS - 1);
+  static constexpr int R1 = 1 << LOGR1;
+  static constexpr int H1 = R1 / 2;                 // pairs per stage-1 group
+  static constexpr int D = N / R1;                  // sub-problem length
+  static constexpr int EPT = N < 32 ? N : 32;       // samples per thread
+  static constexpr int CPT = EPT / 2;               // pairs per thread
+  static constexpr int TPR = N / EPT;               // threads per row (cluster-wide)
+  static constexpr int G1 = EPT / R1;               // stage-1 groups per thread
+  static constexpr int CS = N > 8192 ? N / 8192 : 1;  // CTAs per cluster
+  static constexpr int TPRL = TPR / CS;             // threads per row per CTA
+  static constexpr int ROWS = CS > 1 ? 1 : kThreads / TPR;  // rows per CTA
+  static constexpr int HALF = N / 2;                // slots per row
+  static constexpr int SLOTS = ROWS * HALF / CS;    // slots per CTA
+  // stage s (2..NS): block length and stride in slots
+  __host__ __device__ static constexpr int L(int s) { return D >> (4 * (s - 2)); }
+  __host__ __device__ static constexpr int S(int s) { return L(s) / 16; }
+  // twiddle table offsets (float4 units): stage 1 first, then stages 2..NS
+  __host__ __device__ static constexpr int tw_off(int s)
+  {
+    int off = HALF;
+    for (int k = 2; k < s; ++k) off += L(k);
+    return s == 1 ? 0 : off;
+  }
+  __host__ __device__ static constexpr int tw_size() { return tw_off(NS + 1); }
+};
+
+// ---------------------------------------------------------------------------
+// Packed arithmetic.
+struct cpair { float2 re, im; };
+
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b)
+{
+  unsigned long long d;
+  unsigned long long x = *reinterpret_cast<unsigned long long *>(&a);
+  unsigned long long y = *reinterpret_cast<unsigned long long *>(&b);
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(x), "l"(y));
+  return *reinterpret_cast<float2 *>(&d);
+}
+__device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 f2dup(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ cpair cp_add(cpair a, cpair b) { return {f2add(a.re, b.re), f2add(a.im, b.im)}; }
+__device__ __forceinline__ cpair cp_sub(cpair a, cpair b) { return {f2sub(a.re, b.re), f2sub(a.im, b.im)}; }
+
+// x * (wr + i wi) with per-lane twiddles; CONJ multiplies by the conjugate.
+template <bool CONJ>
+__device__ __forceinline__ cpair cp_mul(cpair x, float2 wr, float2 wi)
+{
+  if (!CONJ)
+    return {f2fma(x.im, f2neg(wi), f2mul(x.re, wr)), f2fma(x.re, wi, f2mul(x.im, wr))};
+  else
+    return {f2fma(x.im, wi, f2mul(x.re, wr)), f2fma(x.re, f2neg(wi), f2mul(x.im, wr))};
+}
+
+__device__ __forceinline__ cpair cp_from4(float4 v) { return {make_float2(v.x, v.y), make_float2(v.z, v.w)}; }
+__device__ __forceinline__ float4 cp_to4(cpair c) { return make_float4(c.re.x, c.re.y, c.im.x, c.im.y); }
+
+// cos(2 pi k / 32) for k in [0, 8], correctly rounded to float.
+__host__ __device__ constexpr float cq32(int k)
+{
+  return k == 0 ? 1.0f : k == 1 ? 0.98078525066375732f : k == 2 ? 0.92387950420379639f
+       : k == 3 ? 0.83146959543228149f : k == 4 ? 0.70710676908493042f
+       : k == 5 ? 0.55557024478912354f : k == 6 ? 0.38268342614173889f
+       : k == 7 ? 0.19509032368659973f : 0.0f;
+}
+// cos and sin of 2 pi k / 32 for k in [0, 16).
+__host__ __device__ constexpr float c32(int k) { return k <= 8 ? cq32(k) : -cq32(16 - k); }
+__host__ __device__ constexpr float s32(int k) { return k <= 8 ? cq32(8 - k) : cq32(k - 8); }
+
+// Multiply a pair by the constant W_32^K = exp(SIGN * 2 pi i K / 32), 0 <= K < 16.
+template <int K, int SIGN>
+__device__ __forceinline__ cpair cp_rot32(cpair x)
+{
+  if (K == 0) return x;
+  constexpr float c = c32(K);
+  constexpr float s = SIGN * s32(K);
+  if (K == 8)  // multiply by SIGN * i
+  {
+    if (SIGN < 0) return {x.im, f2neg(x.re)};
+    else return {f2neg(x.im), x.re};
+  }
+  return {f2fma(x.im, f2dup(-s), f2mul(x.re, f2dup(c))), f2fma(x.re, f2dup(s), f2mul(x.im, f2dup(c)))};
+}
+
+// DIF butterfly b' = (a - b) * W_32^K, a' = a + b.  The +-i case folds the
+// rotation into the subtraction.
+template <int K, int SIGN>
+__device__ __forceinline__ void cp_bfly(cpair &a, cpair &b)
+{
+  cpair s = cp_add(a, b);
+  if (K == 8)
+  {
+    if (SIGN < 0) b = {f2sub(a.im, b.im), f2sub(b.re, a.re)};
+    else b = {f2sub(b.im, a.im), f2sub(a.re, b.re)};
+  }
+  else
+    b = cp_rot32<K, SIGN>(cp_sub(a, b));
+  a = s;
+}
+
+// Radix-2 DIF network over R pairs (lane-parallel): natural-order input,
+// bit-reversed-order output.  c[i] ends up holding X[bitrev_R(i)].
+template <int R, int SIGN, int LEN = R>
+struct DifNet
+{
+  template <int J, int BASE>
+  __device__ __forceinline__ static void level_j(cpair *c)
+  {
+    if constexpr (J < LEN / 2)
+    {
+      cp_bfly<J * (32 / LEN), SIGN>(c[BASE + J], c[BASE + J + LEN / 2]);
+      level_j<J + 1, BASE>(c);
+    }
+  }
+  template <int BASE>
+  __device__ __forceinline__ static void level(cpair *c)
+  {
+    if constexpr (BASE < R)
+    {
+      level_j<0, BASE>(c);
+      level<BASE + LEN>(c);
+    }
+  }
+  __device__ __forceinline__ static void run(cpair *c)
+  {
+    if constexpr (LEN >= 2)
+    {
+      level<0>(c);
+      DifNet<R, SIGN, LEN / 2>::run(c);
+    }
+  }
+};
+
+__host__ __device__ constexpr int bitrev(int i, int bits)
+{
+  int r = 0;
+  for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+  return r;
+}
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+
+// Reverse the 4-bit digits of p (ndig digits).
+__host__ __device__ __forceinline__ int digitrev16(int p, int ndig)
+{
+  int r = 0;
+  for (int d = 0; d < ndig; ++d) { r = (r << 4) | (p & 15); p >>= 4; }
+  return r;
+}
+
+// Shared-memory slot swizzle (16-byte slots, 8 slots per 128-byte bank row).
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 7); }
+
+// ---------------------------------------------------------------------------
+// Launch arguments.
+struct RowArgs
+{
+  const float2 *in;
+  long long in_rs;      // row stride, complex elements
+  float2 *out;
+  long long out_rs;
+  long long rows;
+  const float4 *tw;     // twiddle tables for this length
+  const float4 *rep;    // fused: replica pair table (slot order, scaled 1/N)
+  long long rep_rs;     // fused: replica row stride in slots (0 = one vector)
+  float scale;          // standalone: output scale
+};
+
+enum Mode { kFwd = 0, kInv = 1, kFastconv = 2 };
+
+// Where a slot of the row lives: CTA-local index and owning cluster rank.
+template <class S>
+struct SlotMap
+{
+  __device__ __forceinline__ static int owner(int sigma) { return S::CS > 1 ? sigma / kSlotsPerCta : 0; }
+  __device__ __forceinline__ static int local(int sigma, int rho)
+  {
+    return S::CS > 1 ? (sigma & (kSlotsPerCta - 1)) : rho * S::HALF + sigma;
+  }
+};
+
+// Forward or inverse (conjugate) twiddle load for stage s >= 2: the table
+// stores (w.re, w.re, w.im, w.im) so the load yields both lanes' constants.
+__device__ __forceinline__ void load_tw(const float4 *p, float2 &wr, float2 &wi)
+{
+  float4 v = __ldg(p);
+  wr = make_float2(v.x, v.y);
+  wi = make_float2(v.z, v.w);
+}
+
+template <int LOGN, int MODE>
+__global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
+{
+  using S = Sched<LOGN>;
+  constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
+  extern __shared__ float4 smem[];
+
+  const int t = threadIdx.x;
+  int rank = 0;
+  if constexpr (S::CS > 1) rank = (int)cg::this_cluster().block_rank();
+  const int rho = S::CS > 1 ? 0 : t / S::TPR;                     // row within CTA
+  const int tr = S::CS > 1 ? rank * kThreads + t : t % S::TPR;     // thread within row
+  const long long row = S::CS > 1 ? (long long)(blockIdx.x / S::CS)
+                                  : (long long)blockIdx.x * S::ROWS + rho;
+  const bool active = row < a.rows;
+
+  float4 *peer[S::CS];
+  if constexpr (S::CS > 1)
+  {
+    auto cl = cg::this_cluster();
+#pragma unroll
+    for (int r = 0; r < S::CS; ++r) peer[r] = cl.map_shared_rank(smem, r);
+  }
+  else
+    peer[0] = smem;
+
+  cpair c[S::CPT];
+
+  // ---------------- stage 1 (forward direction SIGN) ----------------
+  {
+    float2 x[S::EPT];
+    const float2 *src = a.in + row * a.in_rs;
+#pragma unroll
+    for (int j = 0; j < S::EPT; ++j)
+      x[j] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int g = 0; g < S::G1; ++g)
+    {
+      cpair *cg1 = c + g * S::H1;
+      // scalar first radix-2 level: lane 0 <- x_r + x_{r+h}, lane 1 <- (x_r - x_{r+h}) W_R1^r
+#pragma unroll
+      for (int r = 0; r < S::H1; ++r)
+      {
+        float2 p = x[g + S::G1 * r], q = x[g + S::G1 * (r + S::H1)];
+        float ur = p.x + q.x, ui = p.y + q.y;
+        float dr = p.x - q.x, di = p.y - q.y;
+        const int k = r * (32 / S::R1);
+        const float wc = c32(k), ws = SIGN * s32(k);
+        float vr, vi;
+        if (k == 0) { vr = dr; vi = di; }
+        else if (k == 8) { vr = SIGN < 0 ? di : -di; vi = SIGN < 0 ? -dr : dr; }
+        else { vr = fmaf(dr, wc, -di * ws); vi = fmaf(dr, ws, di * wc); }
+        cg1[r] = {make_float2(ur, vr), make_float2(ui, vi)};
+      }
+      DifNet<S::H1, SIGN>::run(cg1);
+      const int n = tr + S::TPR * g;
+      if constexpr (S::NS > 1)
+      {
+        // stage-1 twiddles W_N^{n q} (per lane), then pair (q', n) -> slot q'*D + n
+#pragma unroll
+        for (int i = 0; i < S::H1; ++i)
+        {
+          const int qp = bitrev(i, ilog2(S::H1));
+          float4 w = __ldg(a.tw + qp * S::D + n);
+          cg1[i] = (SIGN < 0) ? cp_mul<false>(cg1[i], make_float2(w.x, w.y), make_float2(w.z, w.w))
+                              : cp_mul<true>(cg1[i], make_float2(w.x, w.y), make_float2(w.z, w.w));
+        }
+#pragma unroll
+        for (int i = 0; i < S::H1; ++i)
+        {
+          const int qp = bitrev(i, ilog2(S::H1));
+          const int sigma = qp * S::D + n;
+          peer[SlotMap<S>::owner(sigma)][swz(SlotMap<S>::local(sigma, rho))] = cp_to4(cg1[i]);
+        }
+      }
+    }
+  }
+  if constexpr (S::NS > 1)
+  {
+    if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+  }
+
+  // ---------------- stages 2..NS, forward direction ----------------
+  // One radix-16 group per thread (CPT == 16 whenever NS > 1).
+  auto stage_fwd = [&](auto sc) {
+    constexpr int s = decltype(sc)::value;
+    constexpr int Lg = S::L(s), St = S::S(s);
+    const int g = tr;
+    const int B = g / St, n = g % St;
+    const int base = B * Lg + n;
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+      c[r] = cp_from4(smem[swz(SlotMap<S>::local(base + St * r, rho))]);
+    DifNet<16, SIGN>::run(c);
+#pragma unroll
+    for (int i = 0; i < 16; ++i)
+    {
+      const int q = bitrev(i, 4);
+      if (q != 0 && St > 1)
+      {
+        float2 wr, wi;
+        load_tw(a.tw + S::tw_off(s) + q * St + n, wr, wi);
+        c[i] = (SIGN < 0) ? cp_mul<false>(c[i], wr, wi) : cp_mul<true>(c[i], wr, wi);
+      }
+    }
+    if (s < S::NS)
+    {
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+      {
+        const int q = bitrev(i, 4);
+        smem[swz(SlotMap<S>::local(base + St * q, rho))] = cp_to4(c[i]);
+      }
+    }
+    if (s < S::NS) __syncthreads();
+  };
+  if constexpr (S::NS >= 2) stage_fwd(std::integral_constant<int, 2>{});
+  if constexpr (S::NS >= 3) stage_fwd(std::integral_constant<int, 3>{});
+  if constexpr (S::NS >= 4) stage_fwd(std::integral_constant<int, 4>{});
+
+  if constexpr (MODE != kFastconv)
+  {
+    // ---------------- reorder to natural frequency order and store ----------------
+    // c[] holds the last stage's outputs (never written back).  Pair slot
+    // sigma = q'*D + P holds X[k], X[k+1] with k = 2q' + R1 * digitrev16(P), so it
+    // moves to natural pair index m = q' + (R1/2) * digitrev16(P).
+    cpair v[S::CPT];
+    int dst[S::CPT];
+    if constexpr (S::NS == 1)
+    {
+      // single stage: D == 1, one group per thread, slot index is q'
+#pragma unroll
+      for (int i = 0; i < S::H1; ++i)
+      {
+        v[i] = c[i];
+        dst[i] = bitrev(i, ilog2(S::H1));
+      }
+    }
+    else
+    {
+      constexpr int s = S::NS;
+      constexpr int Lg = S::L(s), St = S::S(s);
+      const int B = tr / St, n = tr % St;
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+      {
+        const int q = bitrev(i, 4);
+        const int sigma = B * Lg + n + St * q;
+        const int qp = sigma / S::D, P = sigma % S::D;
+        v[i] = c[i];
+        dst[i] = qp + S::H1 * digitrev16(P, S::NS - 1);
+      }
+    }
+    if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+#pragma unroll
+    for (int i = 0; i < S::CPT; ++i)
+    {
+      const int m = dst[i];
+      peer[SlotMap<S>::owner(m)][swz(SlotMap<S>::local(m, rho))] = cp_to4(v[i]);
+    }
+    if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+    // natural-order read of this CTA's part of the row, scale, store.
+    const int tl = t % S::TPRL;
+    float2 *dstp = a.out + row * a.out_rs;
+    const float2 sc = f2dup(a.scale);
+#pragma unroll
+    for (int i = 0; i < S::CPT; ++i)
+    {
+      const int l = tl + S::TPRL * i;                       // CTA-local natural pair index
+      const int m = rank * (S::HALF / S::CS) + l;           // row natural pair index
+      cpair p = cp_from4(smem[swz(S::CS > 1 ? l : rho * S::HALF + l)]);
+      p.re = f2mul(p.re, sc);
+      p.im = f2mul(p.im, sc);
+      if (active)
+      {
+        dstp[2 * m] = make_float2(p.re.x, p.im.x);
+        dstp[2 * m + 1] = make_float2(p.re.y, p.im.y);
+      }
+    }
+    return;
+  }
+  else
+  {
+    // ---------------- replica multiply (slot order, 1/N folded in) ----------------
+    const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
+    if constexpr (S::NS == 1)
+    {
+#pragma unroll
+      for (int g = 0; g < S::G1; ++g)
+#pragma unroll
+        for (int i = 0; i < S::H1; ++i)
+        {
+          const int qp = bitrev(i, ilog2(S::H1));
+          float4 w = __ldg(rp + qp * S::D + (tr + S::TPR * g));
+          c[g * S::H1 + i] = cp_mul<false>(c[g * S::H1 + i], make_float2(w.x, w.y), make_float2(w.z, w.w));
+        }
+    }
+    else
+    {
+      constexpr int s = S::NS;
+      constexpr int Lg = S::L(s), St = S::S(s);
+      const int B = tr / St, n = tr % St;
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+      {
+        const int q = bitrev(i, 4);
+        float4 w = __ldg(rp + B * Lg + n + St * q);
+        c[i] = cp_mul<false>(c[i], make_float2(w.x, w.y), make_float2(w.z, w.w));
+      }
+    }
+
+    // ---------------- inverse stages NS..2 (transpose of the forward ones) ----------------
+    // Input z_q sits in c[i] with q = bitrev(i) (the forward output order).
+    auto stage_inv = [&](auto sc) {
+      constexpr int s = decltype(sc)::value;
+      constexpr int Lg = S::L(s), St = S::S(s);
+      const int B = tr / St, n = tr % St;
+      const int base = B * Lg + n;
+      cpair z[16];
+      if (s < S::NS)
+      {
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          z[q] = cp_from4(smem[swz(SlotMap<S>::local(base + St * q, rho))]);
+      }
+      else
+      {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) z[bitrev(i, 4)] = c[i];
+      }
+#pragma unroll
+      for (int q = 1; q < 16; ++q)
+        if (St > 1)
+        {
+          float2 wr, wi;
+          load_tw(a.tw + S::tw_off(s) + q * St + n, wr, wi);
+          z[q] = cp_mul<true>(z[q], wr, wi);
+        }
+      DifNet<16, +1>::run(z);  // z[i] = y[bitrev(i)]
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
+      {
+        const int r = bitrev(i, 4);
+        smem[swz(SlotMap<S>::local(base + St * r, rho))] = cp_to4(z[i]);
+      }
+      if (s > 2) __syncthreads();
+    };
+    if constexpr (S::NS >= 4) stage_inv(std::integral_constant<int, 4>{});
+    if constexpr (S::NS >= 3) stage_inv(std::integral_constant<int, 3>{});
+    if constexpr (S::NS >= 2) stage_inv(std::integral_constant<int, 2>{});
+
+    if constexpr (S::NS > 1)
+    {
+      if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+    }
+
+    // ---------------- inverse stage 1 and store ----------------
+    float2 *dstp = a.out + row * a.out_rs;
+#pragma unroll
+    for (int g = 0; g < S::G1; ++g)
+    {
+      const int n = tr + S::TPR * g;
+      cpair z[S::H1];
+#pragma unroll
+      for (int qp = 0; qp < S::H1; ++qp)
+      {
+        if constexpr (S::NS > 1)
+        {
+          const int sigma = qp * S::D + n;
+          z[qp] = cp_from4(peer[SlotMap<S>::owner(sigma)][swz(SlotMap<S>::local(sigma, rho))]);
+          float4 w = __ldg(a.tw + sigma);
+          z[qp] = cp_mul<true>(z[qp], make_float2(w.x, w.y), make_float2(w.z, w.w));
+        }
+        else
+        {
+          // single stage: forward outputs are still in c in bit-reversed order
+          z[qp] = c[g * S::H1 + bitrev(qp, ilog2(S::H1))];
+        }
+      }
+      DifNet<S::H1, +1>::run(z);  // z[i] = (A_r, B_r) with r = bitrev(i)
+#pragma unroll
+      for (int i = 0; i < S::H1; ++i)
+      {
+        const int r = bitrev(i, ilog2(S::H1));
+        const int k = r * (32 / S::R1);
+        const float wc = c32(k), ws = s32(k);  // conj direction: exp(+2 pi i r / R1)
+        float ar = z[i].re.x, ai = z[i].im.x, br = z[i].re.y, bi = z[i].im.y;
+        float tr_, ti_;
+        if (k == 0) { tr_ = br; ti_ = bi; }
+        else if (k == 8) { tr_ = -bi; ti_ = br; }
+        else { tr_ = fmaf(br, wc, -bi * ws); ti_ = fmaf(br, ws, bi * wc); }
+        if (active)
+        {
+          dstp[n + S::D * r] = make_float2(ar + tr_, ai + ti_);
+          dstp[n + S::D * (r + S::H1)] = make_float2(ar - tr_, ai - ti_);
+        }
+      }
+    }
+    if constexpr (S::CS > 1) cg::this_cluster().sync();
+  }
+}
+
+}  // namespace fcb

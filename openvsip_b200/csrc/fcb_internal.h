@@ -1,0 +1,45 @@
+// Internal declarations shared by the fcb200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace fcb {
+
+struct RowArgs;
+
+// Runtime copy of the compile-time schedule (see Sched<> in fcb_engine.cuh).
+struct SchedRT
+{
+  int logn, n, ns, r1, d, half;
+  long long tw_size;
+};
+SchedRT sched_rt(int logn);
+
+struct KernelInfo
+{
+  const void *fn = nullptr;
+  int cluster = 1;       // CTAs per row (thread-block cluster size)
+  int rows_per_cta = 1;  // rows per CTA when cluster == 1
+  int smem = 0;          // dynamic shared memory per CTA, bytes
+  long long tw_size = 0; // twiddle table entries (float4)
+};
+
+const KernelInfo *kernel_info(int logn, int mode);
+int prepare_kernel(const KernelInfo *k);
+int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaStream_t st);
+
+int build_twiddles(int logn, float4 **out, cudaStream_t st);
+int build_replica_table(int logn, const float2 *spec_dev, long long spec_rs, long long rows,
+                        float4 *rep_dev, cudaStream_t st);
+int replica_spectrum_dev(const float2 *rep_dev, long long n, int matched, float2 *spec_dev,
+                         cudaStream_t st);
+int launch_vmmul(const float2 *v, const float2 *m, long long m_rs, float2 *out, long long out_rs,
+                 long long rows, long long cols, cudaStream_t st);
+int launch_scale_rows(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
+                      const float4 *rep, long long rep_rs, float scale, cudaStream_t st);
+
+int set_error(int code, const char *fmt, ...);
+const char *error_text();
+int cuda_error(cudaError_t e, const char *what);
+
+}  // namespace fcb

@@ -1,0 +1,216 @@
+"""Host-side mirror of the reference's fast-convolution API on the fcb200 backend.
+
+Names and argument meanings follow the reference:
+
+* ``Fftm(rows, cols, direction, scale)`` -- ``vsip::Fftm<complex<float>,
+  complex<float>, row, D, by_reference>`` (src/vsip/impl/signal/fft.hpp:134-161,
+  src/ovxx/signal/fft.hpp:374-436): construct once per domain and scale, then
+  ``fftm(in, out)`` (out of place) or ``fftm(inout)`` (in place); calls may pass
+  fewer rows than planned.
+* ``vmmul(v, m)`` -- ``vsip::vmmul<0>`` (src/vsip/impl/vmmul.hpp:114-128):
+  ``out[r][c] = v[c] * m[r][c]``.
+* ``Fastconv(weights, rows)`` -- the fused expression
+  ``inv_fftm(vmmul<0>(weights, for_fftm(in)))`` with the inverse scaled by 1/N
+  (tests/fastconv.cpp:188-211; benchmarks/fastconv.cpp:100-106).  A weight
+  matrix gives ``inv_fftm(weights * for_fftm(in))`` (tests/fastconv.cpp:213-246).
+
+Arrays are numpy ``complex64`` (host memory, copied through the GPU inside the
+call) or torch ``complex64`` CUDA tensors (device memory; asynchronous on the
+current torch stream).  Rows must be unit-stride.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import FcbError, check, lib
+
+fft_fwd = -2  # reference tag values (src/ovxx/signal/fft/backend.hpp:20-22)
+fft_inv = -1
+
+
+def _exponent(direction: int) -> int:
+    if direction in (fft_fwd, _lib.FCB_FORWARD):
+        return _lib.FCB_FORWARD
+    if direction in (fft_inv, _lib.FCB_INVERSE):
+        return _lib.FCB_INVERSE
+    raise ValueError(f"direction must be fft_fwd or fft_inv, got {direction}")
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _desc(x, writable: bool):
+    """(pointer, rows, cols, row_stride, where) of a 2-D complex64 array/tensor."""
+    if _is_torch(x):
+        import torch
+        if x.dtype != torch.complex64:
+            raise TypeError("expected a complex64 tensor")
+        if not x.is_cuda:
+            raise TypeError("torch tensors must be on a CUDA device; use numpy arrays for host data")
+        if x.dim() == 1:
+            x = x.unsqueeze(0)
+        if x.dim() != 2 or x.stride(1) != 1:
+            raise ValueError("expected a 2-D tensor with unit-stride rows")
+        return x.data_ptr(), x.shape[0], x.shape[1], x.stride(0), _lib.FCB_DEVICE
+    a = x
+    if not isinstance(a, np.ndarray) or a.dtype != np.complex64:
+        raise TypeError("expected a numpy complex64 array")
+    if a.ndim == 1:
+        a = a.reshape(1, -1)
+    if a.ndim != 2 or a.strides[1] != 8 or a.strides[0] % 8:
+        raise ValueError("expected a 2-D array with unit-stride rows")
+    if writable and not a.flags.writeable:
+        raise ValueError("output array is read-only")
+    return a.ctypes.data, a.shape[0], a.shape[1], a.strides[0] // 8, _lib.FCB_HOST
+
+
+def _bind_stream(plan, where) -> None:
+    if where == _lib.FCB_DEVICE:
+        import torch
+        check(lib().fcb_set_stream(plan, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+
+
+def _empty_like(x):
+    if _is_torch(x):
+        import torch
+        return torch.empty_like(x, memory_format=torch.contiguous_format)
+    return np.empty(x.shape, dtype=np.complex64)
+
+
+class _Plan:
+    _handle = None
+
+    def __del__(self):
+        h, self._handle = self._handle, None
+        if h is not None and lib is not None:
+            try:
+                lib().fcb_destroy(h)
+            except Exception:
+                pass
+
+    def info(self) -> dict:
+        n = ctypes.c_longlong()
+        cl = ctypes.c_int()
+        rpc = ctypes.c_int()
+        sm = ctypes.c_int()
+        check(lib().fcb_plan_info(self._handle, ctypes.byref(n), ctypes.byref(cl), ctypes.byref(rpc),
+                                  ctypes.byref(sm)))
+        return {"n": n.value, "cluster_ctas": cl.value, "rows_per_cta": rpc.value, "smem_bytes": sm.value}
+
+    def _exec(self, inp, out):
+        ip, r, c, irs, iw = _desc(inp, False)
+        op, r2, c2, ors, ow = _desc(out, True)
+        if (r, c) != (r2, c2):
+            raise ValueError(f"shape mismatch {(r, c)} vs {(r2, c2)}")
+        if c != self.cols:
+            raise ValueError(f"row length {c} != planned {self.cols}")
+        if iw != ow:
+            raise ValueError("input and output must both be host arrays or both device tensors")
+        _bind_stream(self._handle, iw)
+        check(lib().fcb_exec(self._handle, ctypes.c_void_p(ip), irs, ctypes.c_void_p(op), ors, r, iw))
+        return out
+
+    def __call__(self, inp, out=None):
+        """``plan(in, out)`` by reference, ``plan(inout)`` ... see subclasses."""
+        raise NotImplementedError
+
+
+class Fftm(_Plan):
+    """Row-wise multiple FFT on the GPU (vsip::Fftm<C, C, row, D, R>)."""
+
+    def __init__(self, rows: int, cols: int, direction: int = fft_fwd, scale: float = 1.0):
+        self.rows, self.cols = int(rows), int(cols)
+        self.exponent = _exponent(direction)
+        self.scale = float(scale)
+        h = ctypes.c_void_p()
+        check(lib().fcb_plan_fftm(self.cols, self.rows, self.exponent, self.scale, ctypes.byref(h)))
+        self._handle = h
+
+    def __call__(self, inp, out=None):
+        """By reference: ``fftm(in, out)``.  ``fftm(inout, inplace=True)`` is the
+        in-place form; ``fftm(in)`` returns a new result (by value)."""
+        if out is None:
+            out = _empty_like(inp)
+        return self._exec(inp, out)
+
+    def in_place(self, inout):
+        return self._exec(inout, inout)
+
+
+class Fastconv(_Plan):
+    """Fused fast convolution: ``inv_fftm(vmmul<0>(weights, for_fftm(in)))``.
+
+    weights: a replica spectrum vector (kind="spectrum", the vmmul vector of the
+    reference), or a time-domain replica transformed on the GPU in FP64
+    (kind="time": FFT(w); kind="matched": conj(FFT(w))).  A 2-D weights array
+    with one row per data row is the matrix-of-coefficients form."""
+
+    _KINDS = {"spectrum": _lib.FCB_REPLICA_SPECTRUM, "time": _lib.FCB_REPLICA_TIME,
+              "matched": _lib.FCB_REPLICA_TIME_MATCHED}
+
+    def __init__(self, weights, rows: int, kind: str = "spectrum"):
+        if kind not in self._KINDS:
+            raise ValueError(f"kind must be one of {sorted(self._KINDS)}")
+        if not _is_torch(weights):
+            weights = np.ascontiguousarray(weights, dtype=np.complex64)
+        wp, wr, wc, wrs, ww = _desc(weights, False)
+        self.rows, self.cols = int(rows), int(wc)
+        self.replica_rows = wr
+        h = ctypes.c_void_p()
+        check(lib().fcb_plan_fastconv(self.cols, self.rows, ctypes.c_void_p(wp), wr, wrs,
+                                      self._KINDS[kind], ww, ctypes.byref(h)))
+        self._handle = h
+
+    def __call__(self, inp, out=None):
+        if out is None:
+            out = _empty_like(inp)
+        return self._exec(inp, out)
+
+    def in_place(self, inout):
+        return self._exec(inout, inout)
+
+
+def vmmul(v, m, out=None):
+    """vmmul<0>(v, m): out[r][c] = v[c] * m[r][c], on the GPU.
+
+    v and m must be CUDA complex64 tensors (device data); the op is queued on
+    the current torch stream."""
+    import torch
+    if not (_is_torch(v) and _is_torch(m) and v.is_cuda and m.is_cuda):
+        raise TypeError("vmmul runs on the GPU: pass CUDA complex64 tensors")
+    if out is None:
+        out = torch.empty_like(m)
+    mp, r, c, mrs, _ = _desc(m, False)
+    op, r2, c2, ors, _ = _desc(out, True)
+    v = v.contiguous()
+    if v.numel() != c or (r2, c2) != (r, c):
+        raise ValueError("shape mismatch")
+    stream = torch.cuda.current_stream().cuda_stream
+    check(lib().fcb_vmmul_rows(ctypes.c_void_p(v.data_ptr()), ctypes.c_void_p(mp), mrs, ctypes.c_void_p(op),
+                               ors, r, c, ctypes.c_void_p(stream)))
+    return out
+
+
+def replica_spectrum(replica, matched: bool = True):
+    """FP64-on-GPU spectrum of a time-domain replica (CUDA complex64 tensor)."""
+    import torch
+    if not (_is_torch(replica) and replica.is_cuda):
+        raise TypeError("pass a CUDA complex64 tensor")
+    r = replica.contiguous().reshape(-1)
+    out = torch.empty_like(r)
+    torch.cuda.current_stream().synchronize()
+    check(lib().fcb_replica_spectrum(ctypes.c_void_p(r.data_ptr()), r.numel(), int(bool(matched)),
+                                     ctypes.c_void_p(out.data_ptr())))
+    return out
+
+
+def supported_length(n: int) -> bool:
+    return bool(lib().fcb_supported_length(int(n)))
+
+
+__all__ = ["Fftm", "Fastconv", "vmmul", "replica_spectrum", "supported_length", "fft_fwd", "fft_inv",
+           "FcbError"]
