@@ -1,0 +1,340 @@
+"""Benchmark of the fused fast convolution (pulse compression) on B200.
+
+Workload (one GPU): a single large fast convolution, 1024 pulses x 16384
+samples complex<float>, complex Gaussian noise plus 8 LFM echoes per pulse,
+matched replica of TBP 500.  One step = one fused forward-FFT x replica x
+inverse-FFT pass over that batch, inputs resident in HBM (256 MB read+write per
+step, larger than the 126 MB L2; two input buffers alternate).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 is launched by torchrun (one rank per GPU); every rank runs its own
+batch (weak scaling, no data-path collective), timing is the max over ranks.
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PULSES, NSAMP, TBP, ECHOES = 1024, 16384, 500.0, 8
+WORKLOAD = f"single large fastconv, {PULSES} pulses x {NSAMP} samples complex<float>, {ECHOES} echoes/pulse, LFM TBP {TBP:g}"
+
+
+def baseline_metric():
+    try:
+        with open(os.path.join(ROOT, "BASELINE.json")) as f:
+            return json.load(f)["metric"]
+    except Exception:
+        return "fastconv complex samples/sec"
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "fastconv_1024x16384_ncu.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x1: "gpu_idle"}
+
+    def __init__(self, device_index: int):
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                break
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.nv:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(rows_per_proc: int = 1):
+    """The reference library's own CPU path (oracle/_ref, generic DFT backend --
+    FFTW3 is not installed) on a bounded sample: nproc processes, each running
+    the phased fast convolution on rows_per_proc rows of NSAMP samples."""
+    driver = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+    cores = os.cpu_count() or 1
+    if not os.path.exists(driver):
+        return None
+    t0 = time.perf_counter()
+    procs = [subprocess.Popen([driver, "bench", str(rows_per_proc), str(NSAMP), "1"], stdout=subprocess.PIPE,
+                              text=True) for _ in range(cores)]
+    outs = [json.loads(p.communicate()[0]) for p in procs]
+    wall = time.perf_counter() - t0
+    samples = sum(o["samples"] for o in outs)
+    return {"value": samples / wall, "unit": "complex samples/s", "cores": cores, "kind": "reference",
+            "sample": f"{cores} processes x {rows_per_proc} row x {NSAMP} samples of the workload, phased "
+                      f"Fftm->vmmul->Fftm through the reference's own vsip API, generic FP64 DFT backend "
+                      f"(FFTW3 not installed; O(N^2)), harness-level process parallelism",
+            "seconds": wall}
+
+
+def cpu_port_sample():
+    """Fallback when oracle/_ref is absent: the oracle's FP32 radix-2 port."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    rows = 16 * cores
+    rng = np.random.default_rng(0)
+    x = (rng.standard_normal((rows, NSAMP)) + 1j * rng.standard_normal((rows, NSAMP))).astype(np.complex64)
+    rep = np.ones(NSAMP, dtype=np.complex64)
+    chunks = np.array_split(np.arange(rows), cores)
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=oracle.fastconv_f32, args=(x[c[0]:c[-1] + 1], rep)) for c in chunks]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    wall = time.perf_counter() - t0
+    return {"value": rows * NSAMP / wall, "unit": "complex samples/s", "cores": cores, "kind": "port",
+            "sample": f"{rows} rows x {NSAMP} samples, oracle FP32 radix-2 port, {cores} threads"}
+
+
+def fftw_standin():
+    """scipy.fft complex64 (pocketfft) with all workers: a labelled stand-in for
+    the reference's FFTW3 FP32 path, which is not installed."""
+    import scipy.fft
+    cores = os.cpu_count() or 1
+    rows = 256
+    rng = np.random.default_rng(0)
+    x = (rng.standard_normal((rows, NSAMP)) + 1j * rng.standard_normal((rows, NSAMP))).astype(np.complex64)
+    rep = np.ones(NSAMP, dtype=np.complex64)
+    scipy.fft.ifft(scipy.fft.fft(x[:8], axis=1, workers=cores) * rep, axis=1, workers=cores)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        scipy.fft.ifft(scipy.fft.fft(x, axis=1, workers=cores) * rep, axis=1, workers=cores)
+    wall = (time.perf_counter() - t0) / 3
+    return {"value": rows * NSAMP / wall, "unit": "complex samples/s", "cores": cores,
+            "what": "scipy.fft complex64 fft -> multiply -> ifft, FFTW3 stand-in (not the reference)"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps = []
+    cores = os.cpu_count() or 1
+    kind = "reference"
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_sample(1)
+        if r is None:
+            r = cpu_port_sample()
+            kind = "port"
+        if i >= args.warmup:
+            steps.append(r)
+    value = statistics.median(s["value"] for s in steps)
+    ms = statistics.median(s.get("seconds", 0.0) for s in steps) * 1e3
+    line = {"impl": "reference", "metric": baseline_metric(), "value": value, "unit": "complex samples/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " (bounded sample per step)", "parallelism": f"{cores} host processes"},
+            "cpu_baseline": {"value": value, "unit": "complex samples/s", "cores": cores, "kind": kind,
+                             "sample": steps[-1]["sample"]},
+            "e2e": {"value": value, "unit": "complex samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="fcb", choices=["fcb", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import openvsip_b200 as ov
+    from openvsip_b200 import synth
+
+    job = synth.large_fastconv(seed=1000 + rank, pulses=PULSES, n=NSAMP, tbp=TBP, echoes=ECHOES)
+    x_host = job["data"]
+    rep = job["replica_spectrum"]
+    fc = ov.Fastconv(rep, PULSES)
+    info = fc.info()
+    xin = [torch.from_numpy(x_host).cuda(), torch.from_numpy(np.roll(x_host, 1, axis=0)).cuda()]
+    yout = torch.empty_like(xin[0])
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for i in range(args.warmup):
+        fc(xin[i % 2], yout)
+    torch.cuda.synchronize()
+
+    # accuracy of this run's output on a sample of rows (numpy FP64 FFT)
+    fc(xin[0], yout)
+    torch.cuda.synchronize()
+    ys = yout[:32].cpu().numpy().astype(np.complex128)
+    xs = x_host[:32].astype(np.complex128)
+    ref = np.fft.ifft(np.fft.fft(xs, axis=1) * rep.astype(np.complex128), axis=1)
+    rel = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t_start.record(stream)
+        for i in range(args.steps):
+            starts[i].record(stream)
+            fc(xin[i % 2], yout)
+            ends[i].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    total_ms = t_start.elapsed_time(t_end)
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    t = torch.tensor([total_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+
+    samples_step = PULSES * NSAMP
+    value = samples_step * args.steps * world / (total_ms / 1e3)
+    launch_ms = sum(step_ms) / len(step_ms)
+    alg_bytes = 16.0 * samples_step + 8.0 * NSAMP
+    achieved = alg_bytes / (launch_ms / 1e3) / 1e9
+    peak, peak_src = measured_peak()
+
+    # end to end through the public API with pinned host buffers
+    hin = torch.from_numpy(x_host).pin_memory().numpy()
+    hout = torch.empty(x_host.shape, dtype=torch.complex64).pin_memory().numpy()
+    fc(hin, hout)
+    barrier()
+    e2e_steps = min(args.steps, args.e2e_steps)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fc(hin, hout)
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = samples_step * e2e_steps * world / float(te.item())
+
+    if rank == 0:
+        cpu = None
+        standin = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_reference_sample(1) or cpu_port_sample()
+            cpu.pop("seconds", None)
+            standin = fftw_standin()
+        sorted_ms = sorted(step_ms)
+        line = {
+            "metric": baseline_metric(), "value": value, "unit": "complex samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic (seeded complex Gaussian + LFM echoes)",
+            "config": {"workload": WORKLOAD, "pulses": PULSES, "samples": NSAMP, "tbp": TBP,
+                       "parallelism": f"{world} independent batches (weak)",
+                       "l2": "inputs larger than L2 (256 MB read+write per step, 2 alternating inputs)",
+                       "kernel": {"cluster_ctas": info["cluster_ctas"], "smem_bytes": info["smem_bytes"]}},
+            "latency_ms": {"p50": sorted_ms[len(sorted_ms) // 2],
+                           "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))]},
+            "rel_l2_vs_fp64": rel,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": ncu_traffic(), "peak_source": peak_src,
+                         "alg_bytes_per_launch": alg_bytes, "launch_ms": launch_ms},
+            "cpu_baseline": cpu,
+            "fftw_standin": standin,
+            "e2e": {"value": e2e_value, "unit": "complex samples/s", "h2d_bytes_per_step": x_host.nbytes,
+                    "d2h_bytes_per_step": x_host.nbytes, "steps": e2e_steps,
+                    "how": "Fastconv(host pinned in, host pinned out): chunked H2D/kernel/D2H on 2 streams"},
+            "gpu_launches": args.steps,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -32,11 +32,13 @@ fft_inv = -1
 
 
 def _exponent(direction: int) -> int:
-    if direction in (fft_fwd, _lib.FCB_FORWARD):
+    """Map the reference's direction tag to the transform exponent.  Only the
+    tags are accepted: fft_inv (-1) and the forward exponent (-1) share a value."""
+    if direction == fft_fwd:
         return _lib.FCB_FORWARD
-    if direction in (fft_inv, _lib.FCB_INVERSE):
+    if direction == fft_inv:
         return _lib.FCB_INVERSE
-    raise ValueError(f"direction must be fft_fwd or fft_inv, got {direction}")
+    raise ValueError(f"direction must be fft_fwd ({fft_fwd}) or fft_inv ({fft_inv}), got {direction}")
 
 
 def _is_torch(x) -> bool:

@@ -66,6 +66,8 @@ def test_python_api_validates_types():
     from openvsip_b200 import signal
     with pytest.raises(ValueError):
         signal._exponent(5)
+    assert signal._exponent(signal.fft_fwd) == _lib.FCB_FORWARD
+    assert signal._exponent(signal.fft_inv) == _lib.FCB_INVERSE
     with pytest.raises(TypeError):
         signal._desc(np.zeros((2, 4), dtype=np.complex128), False)
     with pytest.raises(ValueError):
