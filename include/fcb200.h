@@ -112,7 +112,8 @@ FCB_API int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *r
 FCB_API int fcb_exec(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out,
              long long out_rs, long long rows, int where);
 
-/* Use a caller-owned cudaStream_t (NULL = the plan's own stream). */
+/* Queue the plan's device work on a caller-owned cudaStream_t (NULL is the
+ * CUDA default stream).  A new plan uses a private non-blocking stream. */
 FCB_API int fcb_set_stream(fcb_plan plan, void *stream);
 /* Wait for all work queued on the plan's stream. */
 FCB_API int fcb_sync(fcb_plan plan);

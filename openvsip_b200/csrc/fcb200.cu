@@ -46,19 +46,18 @@ SchedRT sched_rt(int logn)
   s.r1 = 1 << (logn - 4 * (s.ns - 1));
   s.d = s.n / s.r1;
   s.half = s.n / 2;
-  int off = s.half;
-  s.tw_size = off;
-  for (int k = 2; k <= s.ns; ++k) s.tw_size += s.d >> (4 * (k - 2));
+  s.tw2_size = 0;
+  for (int k = 2; k <= s.ns; ++k) s.tw2_size += s.d >> (4 * (k - 2));
   return s;
 }
 
 // Twiddle tables in FP64, rounded to float (forward sign; kernels conjugate).
-//   stage 1:   [q'*D + n]          = (W^{n 2q'}.re, W^{n(2q'+1)}.re, W^{n 2q'}.im, W^{n(2q'+1)}.im), W = e^{-2 pi i/N}
-//   stage s:   [off_s + q*S_s + n] = (w.re, w.re, w.im, w.im),  w = e^{-2 pi i n q / L_s}
+//   stage 1 (float4) [q'*D + n] = (W^{n 2q'}.re, W^{n(2q'+1)}.re, W^{n 2q'}.im, W^{n(2q'+1)}.im),
+//                                 W = e^{-2 pi i / N}
+//   stage s >= 2 (float2, after the float4 part) [tw2_off(s) + q*S_s + n] = e^{-2 pi i n q / L_s}
 __global__ void build_tw_kernel(float4 *tw, SchedRT s)
 {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= s.tw_size) return;
   if (i < s.half)
   {
     long long qp = i / s.d, n = i % s.d;
@@ -69,17 +68,19 @@ __global__ void build_tw_kernel(float4 *tw, SchedRT s)
     tw[i] = make_float4((float)c0, (float)c1, (float)s0, (float)s1);
     return;
   }
-  long long off = s.half;
+  long long j = i - s.half;  // float2 index in the stage >= 2 part
+  float2 *tw2 = reinterpret_cast<float2 *>(tw + s.half);
+  long long off = 0;
   for (int k = 2; k <= s.ns; ++k)
   {
     long long L = s.d >> (4 * (k - 2)), St = L / 16;
-    if (i < off + L)
+    if (j < off + L)
     {
-      long long j = i - off, q = j / St, n = j % St;
+      long long jj = j - off, q = jj / St, n = jj % St;
       long long m = (n * q) % L;
       double sn, cs;
       sincospi(-2.0 * (double)m / (double)L, &sn, &cs);
-      tw[i] = make_float4((float)cs, (float)cs, (float)sn, (float)sn);
+      tw2[j] = make_float2((float)cs, (float)sn);
       return;
     }
     off += L;
@@ -173,7 +174,7 @@ static KernelInfo make_info()
   k.cluster = S::CS;
   k.rows_per_cta = S::ROWS;
   k.smem = S::SLOTS * 16;
-  k.tw_size = S::tw_size();
+  k.tw_bytes = S::tw_bytes();
   return k;
 }
 
@@ -237,9 +238,11 @@ int build_twiddles(int logn, float4 **out, cudaStream_t st)
 {
   SchedRT s = sched_rt(logn);
   float4 *tw = nullptr;
-  cudaError_t e = cudaMalloc(&tw, sizeof(float4) * (size_t)s.tw_size);
+  const size_t bytes = 16 * (size_t)s.half + 8 * (size_t)s.tw2_size;
+  cudaError_t e = cudaMalloc(&tw, bytes);
   if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "twiddle table: %s", cudaGetErrorString(e));
-  build_tw_kernel<<<(unsigned)((s.tw_size + 255) / 256), 256, 0, st>>>(tw, s);
+  const long long entries = s.half + s.tw2_size;
+  build_tw_kernel<<<(unsigned)((entries + 255) / 256), 256, 0, st>>>(tw, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) { cudaFree(tw); return cuda_error(e, "twiddle build"); }
   *out = tw;

@@ -125,6 +125,7 @@ int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long
   a.out_rs = out_rs;
   a.rows = rows;
   a.tw = p->tw;
+  a.twi = p->tw;
   a.rep = rep;
   a.rep_rs = rep_rs;
   a.scale = p->scale;
@@ -338,7 +339,7 @@ int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, lon
 int fcb_set_stream(fcb_plan p, void *stream)
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
-  p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+  p->stream = (cudaStream_t)stream;  // NULL is the CUDA default stream, as in CUDA
   return FCB_OK;
 }
 

@@ -71,14 +71,15 @@ struct Sched
   // stage s (2..NS): block length and stride in slots
   __host__ __device__ static constexpr int L(int s) { return D >> (4 * (s - 2)); }
   __host__ __device__ static constexpr int S(int s) { return L(s) / 16; }
-  // twiddle table offsets (float4 units): stage 1 first, then stages 2..NS
-  __host__ __device__ static constexpr int tw_off(int s)
+  // Twiddle tables: stage 1 as HALF float4 entries, then stages 2..NS as
+  // float2 entries at tw2_off(s) (float2 units, counted after the float4 part).
+  __host__ __device__ static constexpr int tw2_off(int s)
   {
-    int off = HALF;
+    int off = 0;
     for (int k = 2; k < s; ++k) off += L(k);
-    return s == 1 ? 0 : off;
+    return off;
   }
-  __host__ __device__ static constexpr int tw_size() { return tw_off(NS + 1); }
+  __host__ __device__ static constexpr int tw_bytes() { return HALF * 16 + tw2_off(NS + 1) * 8; }
 };
 
 // ---------------------------------------------------------------------------
@@ -210,7 +211,66 @@ __host__ __device__ __forceinline__ int digitrev16(int p, int ndig)
 // Shared-memory slot swizzle (16-byte slots, 8 slots per 128-byte bank row).
 __device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 7); }
 
-// ---------------------------------------------------------------------------
+// Loads that stay where they are written: volatile asm is not moved across
+// other volatile asm or memory operations, so twiddle and replica loads are
+// issued in small batches next to their use instead of all being hoisted to
+// the top of the kernel (which would double the live registers).
+__device__ __forceinline__ float4 ldv4(const float4 *p)
+{
+  float4 v;
+  asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float2 ldv2(const float2 *p)
+{
+  float2 v;
+  asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+
+// Shared-memory slot access through 32-bit addresses.  In a cluster, peer
+// CTAs' slots are reached through their shared::cluster window (mapa); a CTA's
+// own shared::cta address is used for its own slots.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t cta_addr, int rank)
+{
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(cta_addr), "r"(rank));
+  return r;
+}
+template <bool CLUSTER>
+__device__ __forceinline__ void st_slot(uint32_t addr, float4 v)
+{
+  if (CLUSTER)
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};"
+                 :: "r"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+  else
+    asm volatile("st.shared.v4.f32 [%0], {%1, %2, %3, %4};"
+                 :: "r"(addr), "f"(v.x), "f"(v.y), "f"(v.z), "f"(v.w) : "memory");
+}
+template <bool CLUSTER>
+__device__ __forceinline__ float4 ld_slot(uint32_t addr)
+{
+  float4 v;
+  if (CLUSTER)
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr) : "memory");
+  else
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ cpair cp_mul4(cpair x, float4 w)  // per-lane (re0, re1, im0, im1)
+{
+  return cp_mul<false>(x, make_float2(w.x, w.y), make_float2(w.z, w.w));
+}
+__device__ __forceinline__ cpair cp_mul4c(cpair x, float4 w)
+{
+  return cp_mul<true>(x, make_float2(w.x, w.y), make_float2(w.z, w.w));
+}
+
 // Launch arguments.
 struct RowArgs
 {
@@ -219,7 +279,11 @@ struct RowArgs
   float2 *out;
   long long out_rs;
   long long rows;
-  const float4 *tw;     // twiddle tables for this length
+  const float4 *tw;     // twiddle tables for this length (see Sched::tw2_off)
+  const float4 *twi;    // the same tables, read by the inverse half of the fused
+                        // kernel: a second pointer keeps the compiler from
+                        // merging those loads with the forward ones and holding
+                        // the forward twiddles in registers across the kernel
   const float4 *rep;    // fused: replica pair table (slot order, scaled 1/N)
   long long rep_rs;     // fused: replica row stride in slots (0 = one vector)
   float scale;          // standalone: output scale
@@ -238,21 +302,18 @@ struct SlotMap
   }
 };
 
-// Forward or inverse (conjugate) twiddle load for stage s >= 2: the table
-// stores (w.re, w.re, w.im, w.im) so the load yields both lanes' constants.
-__device__ __forceinline__ void load_tw(const float4 *p, float2 &wr, float2 &wi)
-{
-  float4 v = __ldg(p);
-  wr = make_float2(v.x, v.y);
-  wi = make_float2(v.z, v.w);
-}
+template <int S_>
+using ic = std::integral_constant<int, S_>;
 
 template <int LOGN, int MODE>
-__global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
+__global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
 {
   using S = Sched<LOGN>;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
+  constexpr int LH1 = ilog2(S::H1);
   extern __shared__ float4 smem[];
+  const float2 *tw2 = reinterpret_cast<const float2 *>(a.tw + S::HALF);
+  const float2 *tw2i = reinterpret_cast<const float2 *>(a.twi + S::HALF);
 
   const int t = threadIdx.x;
   int rank = 0;
@@ -263,29 +324,47 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
                                   : (long long)blockIdx.x * S::ROWS + rho;
   const bool active = row < a.rows;
 
-  float4 *peer[S::CS];
-  if constexpr (S::CS > 1)
+  // 32-bit base address of every cluster rank's slot array (own array when CS == 1)
+  constexpr bool CL = S::CS > 1;
+  uint32_t peer[S::CS];
+  peer[0] = smem_addr(smem);
+  if constexpr (CL)
   {
-    auto cl = cg::this_cluster();
+    const uint32_t own = peer[0];
 #pragma unroll
-    for (int r = 0; r < S::CS; ++r) peer[r] = cl.map_shared_rank(smem, r);
+    for (int r = 0; r < S::CS; ++r) peer[r] = cluster_addr(own, r);
   }
-  else
-    peer[0] = smem;
 
   cpair c[S::CPT];
 
-  // ---------------- stage 1 (forward direction SIGN) ----------------
+  // ---------------- stage 1 (direction SIGN) ----------------
   {
     float2 x[S::EPT];
     const float2 *src = a.in + row * a.in_rs;
 #pragma unroll
     for (int j = 0; j < S::EPT; ++j)
       x[j] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
+    float4 twn[S::H1];
+    if constexpr (S::NS > 1)
+    {
+#pragma unroll
+      for (int i = 0; i < S::H1; ++i) twn[i] = ldv4(a.tw + bitrev(i, LH1) * S::D + tr);
+    }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
     {
       cpair *cg1 = c + g * S::H1;
+      float4 twc[S::H1];
+      if constexpr (S::NS > 1)
+      {
+#pragma unroll
+        for (int i = 0; i < S::H1; ++i) twc[i] = twn[i];
+        if (g + 1 < S::G1)
+        {
+#pragma unroll
+          for (int i = 0; i < S::H1; ++i) twn[i] = ldv4(a.tw + bitrev(i, LH1) * S::D + tr + S::TPR * (g + 1));
+        }
+      }
       // scalar first radix-2 level: lane 0 <- x_r + x_{r+h}, lane 1 <- (x_r - x_{r+h}) W_R1^r
 #pragma unroll
       for (int r = 0; r < S::H1; ++r)
@@ -302,24 +381,16 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
         cg1[r] = {make_float2(ur, vr), make_float2(ui, vi)};
       }
       DifNet<S::H1, SIGN>::run(cg1);
-      const int n = tr + S::TPR * g;
       if constexpr (S::NS > 1)
       {
         // stage-1 twiddles W_N^{n q} (per lane), then pair (q', n) -> slot q'*D + n
+        const int n = tr + S::TPR * g;
 #pragma unroll
         for (int i = 0; i < S::H1; ++i)
         {
-          const int qp = bitrev(i, ilog2(S::H1));
-          float4 w = __ldg(a.tw + qp * S::D + n);
-          cg1[i] = (SIGN < 0) ? cp_mul<false>(cg1[i], make_float2(w.x, w.y), make_float2(w.z, w.w))
-                              : cp_mul<true>(cg1[i], make_float2(w.x, w.y), make_float2(w.z, w.w));
-        }
-#pragma unroll
-        for (int i = 0; i < S::H1; ++i)
-        {
-          const int qp = bitrev(i, ilog2(S::H1));
-          const int sigma = qp * S::D + n;
-          peer[SlotMap<S>::owner(sigma)][swz(SlotMap<S>::local(sigma, rho))] = cp_to4(cg1[i]);
+          cg1[i] = (SIGN < 0) ? cp_mul4(cg1[i], twc[i]) : cp_mul4c(cg1[i], twc[i]);
+          const int sigma = bitrev(i, LH1) * S::D + n;
+          st_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)), cp_to4(cg1[i]));
         }
       }
     }
@@ -329,30 +400,52 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
     if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
   }
 
-  // ---------------- stages 2..NS, forward direction ----------------
-  // One radix-16 group per thread (CPT == 16 whenever NS > 1).
+  // ---------------- stages 2..NS, direction SIGN ----------------
+  // One radix-16 group per thread (CPT == 16 whenever NS > 1).  In the fused
+  // mode the last stage also multiplies by the replica (in two batches).
   auto stage_fwd = [&](auto sc) {
     constexpr int s = decltype(sc)::value;
     constexpr int Lg = S::L(s), St = S::S(s);
-    const int g = tr;
-    const int B = g / St, n = g % St;
+    const int B = tr / St, n = tr % St;
     const int base = B * Lg + n;
 #pragma unroll
     for (int r = 0; r < 16; ++r)
       c[r] = cp_from4(smem[swz(SlotMap<S>::local(base + St * r, rho))]);
-    DifNet<16, SIGN>::run(c);
-#pragma unroll
-    for (int i = 0; i < 16; ++i)
+    float2 w[16];
+    if constexpr (St > 1)
     {
-      const int q = bitrev(i, 4);
-      if (q != 0 && St > 1)
+#pragma unroll
+      for (int q = 1; q < 16; ++q) w[q] = ldv2(tw2 + S::tw2_off(s) + q * St + n);
+    }
+    float4 ra[8];
+    const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
+    if constexpr (MODE == kFastconv && s == S::NS)
+    {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + base + St * bitrev(i, 4));
+    }
+    DifNet<16, SIGN>::run(c);
+    if constexpr (St > 1)
+    {
+#pragma unroll
+      for (int i = 0; i < 16; ++i)
       {
-        float2 wr, wi;
-        load_tw(a.tw + S::tw_off(s) + q * St + n, wr, wi);
-        c[i] = (SIGN < 0) ? cp_mul<false>(c[i], wr, wi) : cp_mul<true>(c[i], wr, wi);
+        const int q = bitrev(i, 4);
+        if (q != 0)
+          c[i] = (SIGN < 0) ? cp_mul<false>(c[i], f2dup(w[q].x), f2dup(w[q].y))
+                            : cp_mul<true>(c[i], f2dup(w[q].x), f2dup(w[q].y));
       }
     }
-    if (s < S::NS)
+    if constexpr (MODE == kFastconv && s == S::NS)
+    {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) c[i] = cp_mul4(c[i], ra[i]);
+#pragma unroll
+      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + base + St * bitrev(8 + i, 4));
+#pragma unroll
+      for (int i = 0; i < 8; ++i) c[8 + i] = cp_mul4(c[8 + i], ra[i]);
+    }
+    if constexpr (s < S::NS)
     {
 #pragma unroll
       for (int i = 0; i < 16; ++i)
@@ -360,12 +453,12 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
         const int q = bitrev(i, 4);
         smem[swz(SlotMap<S>::local(base + St * q, rho))] = cp_to4(c[i]);
       }
+      __syncthreads();
     }
-    if (s < S::NS) __syncthreads();
   };
-  if constexpr (S::NS >= 2) stage_fwd(std::integral_constant<int, 2>{});
-  if constexpr (S::NS >= 3) stage_fwd(std::integral_constant<int, 3>{});
-  if constexpr (S::NS >= 4) stage_fwd(std::integral_constant<int, 4>{});
+  if constexpr (S::NS >= 2) stage_fwd(ic<2>{});
+  if constexpr (S::NS >= 3) stage_fwd(ic<3>{});
+  if constexpr (S::NS >= 4) stage_fwd(ic<4>{});
 
   if constexpr (MODE != kFastconv)
   {
@@ -373,31 +466,21 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
     // c[] holds the last stage's outputs (never written back).  Pair slot
     // sigma = q'*D + P holds X[k], X[k+1] with k = 2q' + R1 * digitrev16(P), so it
     // moves to natural pair index m = q' + (R1/2) * digitrev16(P).
-    cpair v[S::CPT];
     int dst[S::CPT];
     if constexpr (S::NS == 1)
     {
-      // single stage: D == 1, one group per thread, slot index is q'
 #pragma unroll
-      for (int i = 0; i < S::H1; ++i)
-      {
-        v[i] = c[i];
-        dst[i] = bitrev(i, ilog2(S::H1));
-      }
+      for (int i = 0; i < S::H1; ++i) dst[i] = bitrev(i, LH1);  // D == 1: slot index is q'
     }
     else
     {
-      constexpr int s = S::NS;
-      constexpr int Lg = S::L(s), St = S::S(s);
+      constexpr int Lg = S::L(S::NS), St = S::S(S::NS);
       const int B = tr / St, n = tr % St;
 #pragma unroll
       for (int i = 0; i < 16; ++i)
       {
-        const int q = bitrev(i, 4);
-        const int sigma = B * Lg + n + St * q;
-        const int qp = sigma / S::D, P = sigma % S::D;
-        v[i] = c[i];
-        dst[i] = qp + S::H1 * digitrev16(P, S::NS - 1);
+        const int sigma = B * Lg + n + St * bitrev(i, 4);
+        dst[i] = sigma / S::D + S::H1 * digitrev16(sigma % S::D, S::NS - 1);
       }
     }
     if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
@@ -405,7 +488,7 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
     for (int i = 0; i < S::CPT; ++i)
     {
       const int m = dst[i];
-      peer[SlotMap<S>::owner(m)][swz(SlotMap<S>::local(m, rho))] = cp_to4(v[i]);
+      st_slot<CL>(peer[SlotMap<S>::owner(m)] + 16u * swz(SlotMap<S>::local(m, rho)), cp_to4(c[i]));
     }
     if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
     // natural-order read of this CTA's part of the row, scale, store.
@@ -430,43 +513,30 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
   }
   else
   {
-    // ---------------- replica multiply (slot order, 1/N folded in) ----------------
-    const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
     if constexpr (S::NS == 1)
     {
+      // single stage: replica multiply on the stage-1 outputs (slot = q')
+      const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;
 #pragma unroll
-      for (int g = 0; g < S::G1; ++g)
-#pragma unroll
-        for (int i = 0; i < S::H1; ++i)
-        {
-          const int qp = bitrev(i, ilog2(S::H1));
-          float4 w = __ldg(rp + qp * S::D + (tr + S::TPR * g));
-          c[g * S::H1 + i] = cp_mul<false>(c[g * S::H1 + i], make_float2(w.x, w.y), make_float2(w.z, w.w));
-        }
-    }
-    else
-    {
-      constexpr int s = S::NS;
-      constexpr int Lg = S::L(s), St = S::S(s);
-      const int B = tr / St, n = tr % St;
-#pragma unroll
-      for (int i = 0; i < 16; ++i)
+      for (int b0 = 0; b0 < S::H1; b0 += 8)
       {
-        const int q = bitrev(i, 4);
-        float4 w = __ldg(rp + B * Lg + n + St * q);
-        c[i] = cp_mul<false>(c[i], make_float2(w.x, w.y), make_float2(w.z, w.w));
+        constexpr int NB = S::H1 < 8 ? S::H1 : 8;
+        float4 w[NB];
+#pragma unroll
+        for (int i = 0; i < NB; ++i) w[i] = ldv4(rp + bitrev(b0 + i, LH1));
+#pragma unroll
+        for (int i = 0; i < NB; ++i) c[b0 + i] = cp_mul4(c[b0 + i], w[i]);
       }
     }
 
     // ---------------- inverse stages NS..2 (transpose of the forward ones) ----------------
-    // Input z_q sits in c[i] with q = bitrev(i) (the forward output order).
     auto stage_inv = [&](auto sc) {
       constexpr int s = decltype(sc)::value;
       constexpr int Lg = S::L(s), St = S::S(s);
       const int B = tr / St, n = tr % St;
       const int base = B * Lg + n;
       cpair z[16];
-      if (s < S::NS)
+      if constexpr (s < S::NS)
       {
 #pragma unroll
         for (int q = 0; q < 16; ++q)
@@ -477,26 +547,23 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
 #pragma unroll
         for (int i = 0; i < 16; ++i) z[bitrev(i, 4)] = c[i];
       }
+      if constexpr (St > 1)
+      {
+        float2 w[16];
 #pragma unroll
-      for (int q = 1; q < 16; ++q)
-        if (St > 1)
-        {
-          float2 wr, wi;
-          load_tw(a.tw + S::tw_off(s) + q * St + n, wr, wi);
-          z[q] = cp_mul<true>(z[q], wr, wi);
-        }
+        for (int q = 1; q < 16; ++q) w[q] = ldv2(tw2i + S::tw2_off(s) + q * St + n);
+#pragma unroll
+        for (int q = 1; q < 16; ++q) z[q] = cp_mul<true>(z[q], f2dup(w[q].x), f2dup(w[q].y));
+      }
       DifNet<16, +1>::run(z);  // z[i] = y[bitrev(i)]
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-      {
-        const int r = bitrev(i, 4);
-        smem[swz(SlotMap<S>::local(base + St * r, rho))] = cp_to4(z[i]);
-      }
-      if (s > 2) __syncthreads();
+        smem[swz(SlotMap<S>::local(base + St * bitrev(i, 4), rho))] = cp_to4(z[i]);
+      if constexpr (s > 2) __syncthreads();
     };
-    if constexpr (S::NS >= 4) stage_inv(std::integral_constant<int, 4>{});
-    if constexpr (S::NS >= 3) stage_inv(std::integral_constant<int, 3>{});
-    if constexpr (S::NS >= 2) stage_inv(std::integral_constant<int, 2>{});
+    if constexpr (S::NS >= 4) stage_inv(ic<4>{});
+    if constexpr (S::NS >= 3) stage_inv(ic<3>{});
+    if constexpr (S::NS >= 2) stage_inv(ic<2>{});
 
     if constexpr (S::NS > 1)
     {
@@ -505,34 +572,50 @@ __global__ void __launch_bounds__(kThreads, 1) rows_kernel(RowArgs a)
 
     // ---------------- inverse stage 1 and store ----------------
     float2 *dstp = a.out + row * a.out_rs;
+    float4 twn[S::H1];
+    if constexpr (S::NS > 1)
+    {
+#pragma unroll
+      for (int qp = 0; qp < S::H1; ++qp) twn[qp] = ldv4(a.twi + qp * S::D + tr);
+    }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
     {
       const int n = tr + S::TPR * g;
       cpair z[S::H1];
-#pragma unroll
-      for (int qp = 0; qp < S::H1; ++qp)
+      if constexpr (S::NS > 1)
       {
-        if constexpr (S::NS > 1)
+        float4 twc[S::H1];
+#pragma unroll
+        for (int qp = 0; qp < S::H1; ++qp) twc[qp] = twn[qp];
+        if (g + 1 < S::G1)
+        {
+#pragma unroll
+          for (int qp = 0; qp < S::H1; ++qp) twn[qp] = ldv4(a.twi + qp * S::D + n + S::TPR);
+        }
+        float4 v[S::H1];
+#pragma unroll
+        for (int qp = 0; qp < S::H1; ++qp)
         {
           const int sigma = qp * S::D + n;
-          z[qp] = cp_from4(peer[SlotMap<S>::owner(sigma)][swz(SlotMap<S>::local(sigma, rho))]);
-          float4 w = __ldg(a.tw + sigma);
-          z[qp] = cp_mul<true>(z[qp], make_float2(w.x, w.y), make_float2(w.z, w.w));
+          v[qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)));
         }
-        else
-        {
-          // single stage: forward outputs are still in c in bit-reversed order
-          z[qp] = c[g * S::H1 + bitrev(qp, ilog2(S::H1))];
-        }
+#pragma unroll
+        for (int qp = 0; qp < S::H1; ++qp) z[qp] = cp_mul4c(cp_from4(v[qp]), twc[qp]);
+      }
+      else
+      {
+        // single stage: forward outputs are still in c in bit-reversed order
+#pragma unroll
+        for (int qp = 0; qp < S::H1; ++qp) z[qp] = c[g * S::H1 + bitrev(qp, LH1)];
       }
       DifNet<S::H1, +1>::run(z);  // z[i] = (A_r, B_r) with r = bitrev(i)
 #pragma unroll
       for (int i = 0; i < S::H1; ++i)
       {
-        const int r = bitrev(i, ilog2(S::H1));
+        const int r = bitrev(i, LH1);
         const int k = r * (32 / S::R1);
-        const float wc = c32(k), ws = s32(k);  // conj direction: exp(+2 pi i r / R1)
+        const float wc = c32(k), ws = s32(k);  // conjugate direction: exp(+2 pi i r / R1)
         float ar = z[i].re.x, ai = z[i].im.x, br = z[i].re.y, bi = z[i].im.y;
         float tr_, ti_;
         if (k == 0) { tr_ = br; ti_ = bi; }

@@ -11,7 +11,7 @@ struct RowArgs;
 struct SchedRT
 {
   int logn, n, ns, r1, d, half;
-  long long tw_size;
+  long long tw2_size;  // float2 entries of the stage >= 2 twiddle tables
 };
 SchedRT sched_rt(int logn);
 
@@ -21,7 +21,7 @@ struct KernelInfo
   int cluster = 1;       // CTAs per row (thread-block cluster size)
   int rows_per_cta = 1;  // rows per CTA when cluster == 1
   int smem = 0;          // dynamic shared memory per CTA, bytes
-  long long tw_size = 0; // twiddle table entries (float4)
+  long long tw_bytes = 0; // twiddle table size
 };
 
 const KernelInfo *kernel_info(int logn, int mode);

@@ -57,17 +57,19 @@ def _desc(x, writable: bool):
             x = x.unsqueeze(0)
         if x.dim() != 2 or x.stride(1) != 1:
             raise ValueError("expected a 2-D tensor with unit-stride rows")
-        return x.data_ptr(), x.shape[0], x.shape[1], x.stride(0), _lib.FCB_DEVICE
+        rs = x.stride(0) if x.shape[0] > 1 else x.shape[1]
+        return x.data_ptr(), x.shape[0], x.shape[1], rs, _lib.FCB_DEVICE
     a = x
     if not isinstance(a, np.ndarray) or a.dtype != np.complex64:
         raise TypeError("expected a numpy complex64 array")
     if a.ndim == 1:
         a = a.reshape(1, -1)
-    if a.ndim != 2 or a.strides[1] != 8 or a.strides[0] % 8:
+    if a.ndim != 2 or (a.shape[1] > 1 and a.strides[1] != 8) or a.strides[0] % 8:
         raise ValueError("expected a 2-D array with unit-stride rows")
     if writable and not a.flags.writeable:
         raise ValueError("output array is read-only")
-    return a.ctypes.data, a.shape[0], a.shape[1], a.strides[0] // 8, _lib.FCB_HOST
+    rs = a.strides[0] // 8 if a.shape[0] > 1 else a.shape[1]  # one row: any stride is fine
+    return a.ctypes.data, a.shape[0], a.shape[1], rs, _lib.FCB_HOST
 
 
 def _bind_stream(plan, where) -> None:
