@@ -63,7 +63,7 @@ def test_no_device_is_reported():
 
 
 def test_python_api_validates_types():
-    from openvsip_b200 import signal
+    from openvsip_b200 import vsip as signal
     with pytest.raises(ValueError):
         signal._exponent(5)
     assert signal._exponent(signal.fft_fwd) == _lib.FCB_FORWARD
