@@ -212,6 +212,7 @@ def main():
     ap.add_argument("--impl", default="fcb", choices=["fcb", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--threads", type=int, default=0, help="force the 256- or 512-thread kernel variant")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -231,6 +232,8 @@ def main():
     import openvsip_b200 as ov
     from openvsip_b200 import synth
 
+    if args.threads:
+        ov.lib().fcb_tune_set(NSAMP, 2, args.threads)
     job = synth.large_fastconv(seed=1000 + rank, pulses=PULSES, n=NSAMP, tbp=TBP, echoes=ECHOES)
     x_host = job["data"]
     rep = job["replica_spectrum"]
@@ -316,7 +319,8 @@ def main():
             "config": {"workload": WORKLOAD, "pulses": PULSES, "samples": NSAMP, "tbp": TBP,
                        "parallelism": f"{world} independent batches (weak)",
                        "l2": "inputs larger than L2 (256 MB read+write per step, 2 alternating inputs)",
-                       "kernel": {"cluster_ctas": info["cluster_ctas"], "smem_bytes": info["smem_bytes"]}},
+                       "kernel": {"threads": info["threads"], "cluster_ctas": info["cluster_ctas"],
+                                  "smem_bytes": info["smem_bytes"]}},
             "latency_ms": {"p50": sorted_ms[len(sorted_ms) // 2],
                            "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))]},
             "rel_l2_vs_fp64": rel,

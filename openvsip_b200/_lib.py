@@ -68,7 +68,9 @@ SIGNATURES = {
     "fcb_sync": (c_int, [c_vp]),
     "fcb_destroy": (c_int, [c_vp]),
     "fcb_plan_info": (c_int, [c_vp, ctypes.POINTER(c_ll), ctypes.POINTER(c_int), ctypes.POINTER(c_int),
-                              ctypes.POINTER(c_int)]),
+                              ctypes.POINTER(c_int), ctypes.POINTER(c_int)]),
+    "fcb_tune_set": (c_int, [c_ll, c_int, c_int]),
+    "fcb_tune_get": (c_int, [c_ll, c_int]),
     "fcb_vmmul_rows": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_ll, c_vp]),
     "fcb_replica_spectrum": (c_int, [c_vp, c_ll, c_int, c_vp]),
     "fcb_batch_create": (c_int, [c_ll, c_ll, ctypes.POINTER(c_vp)]),

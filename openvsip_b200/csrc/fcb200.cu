@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <mutex>
 
 namespace fcb {
 
@@ -164,40 +165,84 @@ __global__ void scale_rows_kernel(const float2 *in, long long in_rs, float2 *out
 }
 
 // ---------------------------------------------------------------------------
-// Kernel table.
-template <int LOGN, int MODE>
+// Kernel table: [logn][mode][variant], variant 0 = 256-thread CTAs, 1 = 512.
+template <int LOGN, int MODE, int T>
 static KernelInfo make_info()
 {
-  using S = Sched<LOGN>;
+  using S = Sched<LOGN, T>;
   KernelInfo k;
-  k.fn = (const void *)&rows_kernel<LOGN, MODE>;
+  k.fn = (const void *)&rows_kernel<LOGN, MODE, T>;
+  k.threads = T;
   k.cluster = S::CS;
   k.rows_per_cta = S::ROWS;
-  k.smem = S::SLOTS * 16;
+  k.smem = S::SMEM;
   k.tw_bytes = S::tw_bytes();
   return k;
 }
 
+constexpr int kMin512 = 13;  // 512-thread variants exist for rows of 8192 samples and more
+
 template <int LOGN>
-static void fill_table(KernelInfo (*tab)[3])
+static void fill_table(KernelInfo (*tab)[3][2])
 {
   if constexpr (LOGN >= 1)
   {
-    tab[LOGN][kFwd] = make_info<LOGN, kFwd>();
-    tab[LOGN][kInv] = make_info<LOGN, kInv>();
-    tab[LOGN][kFastconv] = make_info<LOGN, kFastconv>();
+    tab[LOGN][kFwd][0] = make_info<LOGN, kFwd, 256>();
+    tab[LOGN][kInv][0] = make_info<LOGN, kInv, 256>();
+    tab[LOGN][kFastconv][0] = make_info<LOGN, kFastconv, 256>();
+    if constexpr (LOGN >= kMin512)
+    {
+      tab[LOGN][kFwd][1] = make_info<LOGN, kFwd, 512>();
+      tab[LOGN][kInv][1] = make_info<LOGN, kInv, 512>();
+      tab[LOGN][kFastconv][1] = make_info<LOGN, kFastconv, 512>();
+    }
     fill_table<LOGN - 1>(tab);
   }
 }
 
-static KernelInfo g_table[kMaxLogN + 1][3];
+static KernelInfo g_table[kMaxLogN + 1][3][2];
 static std::once_flag g_table_once;
+// Variant chosen per (logn, mode); set by the autotuner through fcb_tune_set.
+static int g_variant[kMaxLogN + 1][3];
+static std::mutex g_variant_mu;
+
+static void init_table()
+{
+  std::call_once(g_table_once, [] {
+    fill_table<kMaxLogN>(g_table);
+    for (int l = 0; l <= kMaxLogN; ++l)
+      for (int m = 0; m < 3; ++m)
+        g_variant[l][m] = (l == 14) ? 1 : 0;  // default: one 512-thread CTA per 16384-sample row
+  });
+}
 
 const KernelInfo *kernel_info(int logn, int mode)
 {
-  std::call_once(g_table_once, [] { fill_table<kMaxLogN>(g_table); });
-  if (logn < 1 || logn > kMaxLogN) return nullptr;
-  return &g_table[logn][mode];
+  init_table();
+  if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return nullptr;
+  std::lock_guard<std::mutex> lk(g_variant_mu);
+  return &g_table[logn][mode][g_variant[logn][mode]];
+}
+
+int set_variant(int logn, int mode, int threads)
+{
+  init_table();
+  if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2)
+    return set_error(FCB_ERR_INVALID, "bad length or mode for tuning");
+  int v = threads == 512 ? 1 : threads == 256 ? 0 : -1;
+  if (v < 0) return set_error(FCB_ERR_INVALID, "threads must be 256 or 512");
+  if (v == 1 && logn < kMin512) return set_error(FCB_ERR_UNSUPPORTED, "no 512-thread variant below 8192 samples");
+  std::lock_guard<std::mutex> lk(g_variant_mu);
+  g_variant[logn][mode] = v;
+  return FCB_OK;
+}
+
+int get_variant(int logn, int mode)
+{
+  init_table();
+  if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return 0;
+  std::lock_guard<std::mutex> lk(g_variant_mu);
+  return g_variant[logn][mode] ? 512 : 256;
 }
 
 int prepare_kernel(const KernelInfo *k)
@@ -215,7 +260,7 @@ int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaSt
   if (ctas > 0x7fffffffLL) return set_error(FCB_ERR_INVALID, "too many rows in one call");
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)ctas);
-  cfg.blockDim = dim3(kThreads);
+  cfg.blockDim = dim3(k->threads);
   cfg.dynamicSmemBytes = k->smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];

@@ -358,14 +358,30 @@ int fcb_destroy(fcb_plan p)
   return FCB_OK;
 }
 
-int fcb_plan_info(fcb_plan p, long long *n, int *cluster_ctas, int *rows_per_cta, int *smem_bytes)
+int fcb_plan_info(fcb_plan p, long long *n, int *cluster_ctas, int *rows_per_cta, int *smem_bytes,
+                  int *threads)
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
   if (n) *n = p->n;
+  if (threads) *threads = p->k ? p->k->threads : 0;
   if (cluster_ctas) *cluster_ctas = p->k ? p->k->cluster : 1;
   if (rows_per_cta) *rows_per_cta = p->k ? p->k->rows_per_cta : 1;
   if (smem_bytes) *smem_bytes = p->k ? p->k->smem : 0;
   return FCB_OK;
+}
+
+int fcb_tune_set(long long n, int kind, int threads)
+{
+  int l = log2_exact(n);
+  if (l < 1 || l > kMaxLogN) return set_error(FCB_ERR_UNSUPPORTED, "length %lld has no tunable kernel", n);
+  return set_variant(l, kind, threads);
+}
+
+int fcb_tune_get(long long n, int kind)
+{
+  int l = log2_exact(n);
+  if (l < 1 || l > kMaxLogN || kind < 0 || kind > 2) return 0;
+  return get_variant(l, kind);
 }
 
 int fcb_vmmul_rows(const fcb_cf32 *v, const fcb_cf32 *m, long long m_rs, fcb_cf32 *out, long long out_rs,

@@ -22,17 +22,22 @@
 //  * Stages 2.. are radix-16 DIF steps inside the sub-problem pairs, in place
 //    in a 16-byte-slot shared-memory array (XOR swizzle against bank conflicts).
 //    A thread reads and writes only its own group's slots inside a stage, so
-//    one barrier per exchange suffices.
+//    one barrier per exchange suffices.  Their twiddles are read from a copy
+//    of the tables in shared memory, made once per CTA.
+//  * Stage-1 twiddles W_N^{nq} for the thread's groups n = t + T*g factor into
+//    W_N^{tq} (loaded once per thread) times W_32^{gq} (a compile-time
+//    constant), because N = 32 T.
 //  * After the last forward stage a slot sigma = q'*D + P holds X[k], X[k+1]
 //    with k = 2q' + R1 * digitrev16(P).  The fused path multiplies by a replica
 //    table stored in that order (scaled by 1/N, exact for powers of two) and
 //    runs the exact transpose of the forward stages with conjugate twiddles, so
 //    no reordering pass is ever needed and every row makes one HBM read and one
 //    HBM write.  The standalone FFTs add one reorder exchange.
-//  * Rows of N <= 8192 samples: one CTA of 256 threads holds 8192 samples
-//    (8192/N rows).  N >= 16384: a thread-block cluster of N/8192 CTAs holds one
-//    row; the two exchanges adjacent to stage 1 cross CTAs through distributed
-//    shared memory (stores forward, loads inverse).  No TMA multicast is used.
+//  * A CTA of THREADS threads (256 or 512) holds 32*THREADS samples: several
+//    short rows, one row, or -- for longer rows -- one part of a row, the row
+//    then being spread over a thread-block cluster whose CTAs exchange through
+//    distributed shared memory in the two exchanges next to stage 1 (stores
+//    forward, loads inverse).  No TMA multicast is used anywhere.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -44,15 +49,14 @@ namespace fcb {
 
 namespace cg = cooperative_groups;
 
-constexpr int kThreads = 256;        // threads per CTA
-constexpr int kSlotsPerCta = 4096;   // 16-byte slots (complex pairs) per CTA
 constexpr int kMaxLogN = 16;
 
 // ---------------------------------------------------------------------------
-// Schedule of a length-2^LOGN row transform.
-template <int LOGN>
+// Schedule of a length-2^LOGN row transform on CTAs of THREADS threads.
+template <int LOGN, int THREADS>
 struct Sched
 {
+  static constexpr int T = THREADS;
   static constexpr int N = 1 << LOGN;
   static constexpr int NS = (LOGN <= 5) ? 1 : 1 + (LOGN - 5 + 3) / 4;  // stages
   static constexpr int LOGR1 = LOGN - 4 * (NS - 1);
@@ -63,16 +67,19 @@ struct Sched
   static constexpr int CPT = EPT / 2;               // pairs per thread
   static constexpr int TPR = N / EPT;               // threads per row (cluster-wide)
   static constexpr int G1 = EPT / R1;               // stage-1 groups per thread
-  static constexpr int CS = N > 8192 ? N / 8192 : 1;  // CTAs per cluster
-  static constexpr int TPRL = TPR / CS;             // threads per row per CTA
-  static constexpr int ROWS = CS > 1 ? 1 : kThreads / TPR;  // rows per CTA
+  static constexpr int SPC = T * 16;                // slots per CTA for rows of >= 32 samples
   static constexpr int HALF = N / 2;                // slots per row
-  static constexpr int SLOTS = ROWS * HALF / CS;    // slots per CTA
+  static constexpr int CS = HALF > SPC ? HALF / SPC : 1;  // CTAs per cluster
+  static constexpr int TPRL = TPR / CS;             // threads per row per CTA
+  static constexpr int ROWS = CS > 1 ? 1 : T / TPR; // rows per CTA
+  static constexpr int SLOTS = CS > 1 ? SPC : ROWS * HALF;  // slots per CTA
   // stage s (2..NS): block length and stride in slots
   __host__ __device__ static constexpr int L(int s) { return D >> (4 * (s - 2)); }
   __host__ __device__ static constexpr int S(int s) { return L(s) / 16; }
-  // Twiddle tables: stage 1 as HALF float4 entries, then stages 2..NS as
-  // float2 entries at tw2_off(s) (float2 units, counted after the float4 part).
+  // Twiddle tables in global memory: stage 1 as HALF float4 entries, then
+  // stages 2..NS as float2 entries at tw2_off(s) (float2 units, counted after
+  // the float4 part).  Stages 2..NS-1 (the ones with twiddles) are copied to
+  // shared memory after the slot array.
   __host__ __device__ static constexpr int tw2_off(int s)
   {
     int off = 0;
@@ -80,7 +87,10 @@ struct Sched
     return off;
   }
   __host__ __device__ static constexpr int tw_bytes() { return HALF * 16 + tw2_off(NS + 1) * 8; }
+  static constexpr int TWS = NS >= 3 ? tw2_off(NS) : 0;   // float2 entries kept in shared memory
+  static constexpr int SMEM = SLOTS * 16 + TWS * 8;
 };
+
 
 // ---------------------------------------------------------------------------
 // Packed arithmetic.
@@ -124,9 +134,11 @@ __host__ __device__ constexpr float cq32(int k)
        : k == 5 ? 0.55557024478912354f : k == 6 ? 0.38268342614173889f
        : k == 7 ? 0.19509032368659973f : 0.0f;
 }
-// cos and sin of 2 pi k / 32 for k in [0, 16).
-__host__ __device__ constexpr float c32(int k) { return k <= 8 ? cq32(k) : -cq32(16 - k); }
-__host__ __device__ constexpr float s32(int k) { return k <= 8 ? cq32(8 - k) : cq32(k - 8); }
+// cos and sin of 2 pi k / 32 for k in [0, 32).
+__host__ __device__ constexpr float c32h(int k) { return k <= 8 ? cq32(k) : -cq32(16 - k); }
+__host__ __device__ constexpr float s32h(int k) { return k <= 8 ? cq32(8 - k) : cq32(k - 8); }
+__host__ __device__ constexpr float c32(int k) { return k < 16 ? c32h(k) : -c32h(k - 16); }
+__host__ __device__ constexpr float s32(int k) { return k < 16 ? s32h(k) : -s32h(k - 16); }
 
 // Multiply a pair by the constant W_32^K = exp(SIGN * 2 pi i K / 32), 0 <= K < 16.
 template <int K, int SIGN>
@@ -222,16 +234,10 @@ __device__ __forceinline__ float4 ldv4(const float4 *p)
                : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
   return v;
 }
-__device__ __forceinline__ float2 ldv2(const float2 *p)
-{
-  float2 v;
-  asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
-  return v;
-}
 
-// Shared-memory slot access through 32-bit addresses.  In a cluster, peer
-// CTAs' slots are reached through their shared::cluster window (mapa); a CTA's
-// own shared::cta address is used for its own slots.
+// Shared-memory access through 32-bit addresses.  In a cluster, peer CTAs'
+// slots are reached through their shared::cluster window (mapa); a CTA's own
+// shared::cta address is used for its own slots.
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ uint32_t cluster_addr(uint32_t cta_addr, int rank)
 {
@@ -261,6 +267,12 @@ __device__ __forceinline__ float4 ld_slot(uint32_t addr)
                  : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr) : "memory");
   return v;
 }
+__device__ __forceinline__ float2 ld_tw(uint32_t addr)
+{
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
+  return v;
+}
 
 __device__ __forceinline__ cpair cp_mul4(cpair x, float4 w)  // per-lane (re0, re1, im0, im1)
 {
@@ -269,6 +281,17 @@ __device__ __forceinline__ cpair cp_mul4(cpair x, float4 w)  // per-lane (re0, r
 __device__ __forceinline__ cpair cp_mul4c(cpair x, float4 w)
 {
   return cp_mul<true>(x, make_float2(w.x, w.y), make_float2(w.z, w.w));
+}
+// Per-lane constant rotation: lane 0 by W_32^{k0}, lane 1 by W_32^{k1}, with
+// W_32 = exp(SIGN 2 pi i / 32).  k0, k1 are compile-time constants after
+// unrolling, so the cos/sin pairs fold to immediates.
+template <int SIGN>
+__device__ __forceinline__ cpair cp_rot2(cpair x, int k0, int k1)
+{
+  if (k0 == 0 && k1 == 0) return x;
+  const float2 c = make_float2(c32(k0), c32(k1));
+  const float2 s = make_float2(SIGN * s32(k0), SIGN * s32(k1));
+  return {f2fma(x.im, f2neg(s), f2mul(x.re, c)), f2fma(x.re, s, f2mul(x.im, c))};
 }
 
 // Launch arguments.
@@ -291,41 +314,39 @@ struct RowArgs
 
 enum Mode { kFwd = 0, kInv = 1, kFastconv = 2 };
 
-// Where a slot of the row lives: CTA-local index and owning cluster rank.
+// Where a slot of the row lives: owning cluster rank and CTA-local index.
 template <class S>
 struct SlotMap
 {
-  __device__ __forceinline__ static int owner(int sigma) { return S::CS > 1 ? sigma / kSlotsPerCta : 0; }
+  __device__ __forceinline__ static int owner(int sigma) { return S::CS > 1 ? sigma / S::SPC : 0; }
   __device__ __forceinline__ static int local(int sigma, int rho)
   {
-    return S::CS > 1 ? (sigma & (kSlotsPerCta - 1)) : rho * S::HALF + sigma;
+    return S::CS > 1 ? (sigma & (S::SPC - 1)) : rho * S::HALF + sigma;
   }
 };
 
 template <int S_>
 using ic = std::integral_constant<int, S_>;
 
-template <int LOGN, int MODE>
-__global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
+template <int LOGN, int MODE, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
 {
-  using S = Sched<LOGN>;
+  using S = Sched<LOGN, THREADS>;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
   constexpr int LH1 = ilog2(S::H1);
+  constexpr bool CL = S::CS > 1;
   extern __shared__ float4 smem[];
   const float2 *tw2 = reinterpret_cast<const float2 *>(a.tw + S::HALF);
-  const float2 *tw2i = reinterpret_cast<const float2 *>(a.twi + S::HALF);
 
   const int t = threadIdx.x;
   int rank = 0;
-  if constexpr (S::CS > 1) rank = (int)cg::this_cluster().block_rank();
-  const int rho = S::CS > 1 ? 0 : t / S::TPR;                     // row within CTA
-  const int tr = S::CS > 1 ? rank * kThreads + t : t % S::TPR;     // thread within row
-  const long long row = S::CS > 1 ? (long long)(blockIdx.x / S::CS)
-                                  : (long long)blockIdx.x * S::ROWS + rho;
+  if constexpr (CL) rank = (int)cg::this_cluster().block_rank();
+  const int rho = CL ? 0 : t / S::TPR;                       // row within CTA
+  const int tr = CL ? rank * THREADS + t : t % S::TPR;       // thread within row
+  const long long row = CL ? (long long)(blockIdx.x / S::CS) : (long long)blockIdx.x * S::ROWS + rho;
   const bool active = row < a.rows;
 
   // 32-bit base address of every cluster rank's slot array (own array when CS == 1)
-  constexpr bool CL = S::CS > 1;
   uint32_t peer[S::CS];
   peer[0] = smem_addr(smem);
   if constexpr (CL)
@@ -333,6 +354,19 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
     const uint32_t own = peer[0];
 #pragma unroll
     for (int r = 0; r < S::CS; ++r) peer[r] = cluster_addr(own, r);
+  }
+  const uint32_t slot_base = smem_addr(smem);
+  const uint32_t tw_base = slot_base + 16u * S::SLOTS;  // later-stage twiddles in shared memory
+  auto slot_addr = [&](int local) { return slot_base + 16u * (uint32_t)swz(local); };
+
+  // copy the twiddle tables of stages 2..NS-1 to shared memory (read before
+  // the first barrier below, used after it)
+  if constexpr (S::TWS > 0)
+  {
+    const float4 *src = reinterpret_cast<const float4 *>(tw2);
+    float4 *dst = reinterpret_cast<float4 *>(smem + S::SLOTS);
+#pragma unroll 4
+    for (int i = t; i < S::TWS / 2; i += THREADS) dst[i] = __ldg(src + i);
   }
 
   cpair c[S::CPT];
@@ -344,27 +378,17 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
 #pragma unroll
     for (int j = 0; j < S::EPT; ++j)
       x[j] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
-    float4 twn[S::H1];
+    // W_N^{tr q} for q = 2q' + lane; groups g > 0 add the constant W_32^{g q}
+    float4 tw1[S::H1];
     if constexpr (S::NS > 1)
     {
 #pragma unroll
-      for (int i = 0; i < S::H1; ++i) twn[i] = ldv4(a.tw + bitrev(i, LH1) * S::D + tr);
+      for (int i = 0; i < S::H1; ++i) tw1[i] = ldv4(a.tw + bitrev(i, LH1) * S::D + tr);
     }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
     {
       cpair *cg1 = c + g * S::H1;
-      float4 twc[S::H1];
-      if constexpr (S::NS > 1)
-      {
-#pragma unroll
-        for (int i = 0; i < S::H1; ++i) twc[i] = twn[i];
-        if (g + 1 < S::G1)
-        {
-#pragma unroll
-          for (int i = 0; i < S::H1; ++i) twn[i] = ldv4(a.tw + bitrev(i, LH1) * S::D + tr + S::TPR * (g + 1));
-        }
-      }
       // scalar first radix-2 level: lane 0 <- x_r + x_{r+h}, lane 1 <- (x_r - x_{r+h}) W_R1^r
 #pragma unroll
       for (int r = 0; r < S::H1; ++r)
@@ -388,16 +412,18 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
 #pragma unroll
         for (int i = 0; i < S::H1; ++i)
         {
-          cg1[i] = (SIGN < 0) ? cp_mul4(cg1[i], twc[i]) : cp_mul4c(cg1[i], twc[i]);
-          const int sigma = bitrev(i, LH1) * S::D + n;
-          st_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)), cp_to4(cg1[i]));
+          const int qp = bitrev(i, LH1);
+          cpair v = (SIGN < 0) ? cp_mul4(cg1[i], tw1[i]) : cp_mul4c(cg1[i], tw1[i]);
+          v = cp_rot2<SIGN>(v, (g * 2 * qp) & 31, (g * (2 * qp + 1)) & 31);
+          const int sigma = qp * S::D + n;
+          st_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)), cp_to4(v));
         }
       }
     }
   }
   if constexpr (S::NS > 1)
   {
-    if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+    if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
   }
 
   // ---------------- stages 2..NS, direction SIGN ----------------
@@ -408,17 +434,11 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
     constexpr int Lg = S::L(s), St = S::S(s);
     const int B = tr / St, n = tr % St;
     const int base = B * Lg + n;
+    const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
 #pragma unroll
     for (int r = 0; r < 16; ++r)
-      c[r] = cp_from4(smem[swz(SlotMap<S>::local(base + St * r, rho))]);
-    float2 w[16];
-    if constexpr (St > 1)
-    {
-#pragma unroll
-      for (int q = 1; q < 16; ++q) w[q] = ldv2(tw2 + S::tw2_off(s) + q * St + n);
-    }
+      c[r] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * r, rho))));
     float4 ra[8];
-    const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
     if constexpr (MODE == kFastconv && s == S::NS)
     {
 #pragma unroll
@@ -427,6 +447,9 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
     DifNet<16, SIGN>::run(c);
     if constexpr (St > 1)
     {
+      float2 w[16];
+#pragma unroll
+      for (int q = 1; q < 16; ++q) w[q] = ld_tw(tw_base + 8u * (S::tw2_off(s) + q * St + n));
 #pragma unroll
       for (int i = 0; i < 16; ++i)
       {
@@ -449,10 +472,7 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
     {
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-      {
-        const int q = bitrev(i, 4);
-        smem[swz(SlotMap<S>::local(base + St * q, rho))] = cp_to4(c[i]);
-      }
+        st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, 4), rho)), cp_to4(c[i]));
       __syncthreads();
     }
   };
@@ -483,14 +503,14 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
         dst[i] = sigma / S::D + S::H1 * digitrev16(sigma % S::D, S::NS - 1);
       }
     }
-    if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+    if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
 #pragma unroll
     for (int i = 0; i < S::CPT; ++i)
     {
       const int m = dst[i];
       st_slot<CL>(peer[SlotMap<S>::owner(m)] + 16u * swz(SlotMap<S>::local(m, rho)), cp_to4(c[i]));
     }
-    if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+    if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
     // natural-order read of this CTA's part of the row, scale, store.
     const int tl = t % S::TPRL;
     float2 *dstp = a.out + row * a.out_rs;
@@ -500,7 +520,7 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
     {
       const int l = tl + S::TPRL * i;                       // CTA-local natural pair index
       const int m = rank * (S::HALF / S::CS) + l;           // row natural pair index
-      cpair p = cp_from4(smem[swz(S::CS > 1 ? l : rho * S::HALF + l)]);
+      cpair p = cp_from4(ld_slot<false>(slot_addr(CL ? l : rho * S::HALF + l)));
       p.re = f2mul(p.re, sc);
       p.im = f2mul(p.im, sc);
       if (active)
@@ -517,10 +537,10 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
     {
       // single stage: replica multiply on the stage-1 outputs (slot = q')
       const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;
+      constexpr int NB = S::H1 < 8 ? S::H1 : 8;
 #pragma unroll
-      for (int b0 = 0; b0 < S::H1; b0 += 8)
+      for (int b0 = 0; b0 < S::H1; b0 += NB)
       {
-        constexpr int NB = S::H1 < 8 ? S::H1 : 8;
         float4 w[NB];
 #pragma unroll
         for (int i = 0; i < NB; ++i) w[i] = ldv4(rp + bitrev(b0 + i, LH1));
@@ -540,7 +560,7 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
       {
 #pragma unroll
         for (int q = 0; q < 16; ++q)
-          z[q] = cp_from4(smem[swz(SlotMap<S>::local(base + St * q, rho))]);
+          z[q] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * q, rho))));
       }
       else
       {
@@ -551,14 +571,14 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
       {
         float2 w[16];
 #pragma unroll
-        for (int q = 1; q < 16; ++q) w[q] = ldv2(tw2i + S::tw2_off(s) + q * St + n);
+        for (int q = 1; q < 16; ++q) w[q] = ld_tw(tw_base + 8u * (S::tw2_off(s) + q * St + n));
 #pragma unroll
         for (int q = 1; q < 16; ++q) z[q] = cp_mul<true>(z[q], f2dup(w[q].x), f2dup(w[q].y));
       }
       DifNet<16, +1>::run(z);  // z[i] = y[bitrev(i)]
 #pragma unroll
       for (int i = 0; i < 16; ++i)
-        smem[swz(SlotMap<S>::local(base + St * bitrev(i, 4), rho))] = cp_to4(z[i]);
+        st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, 4), rho)), cp_to4(z[i]));
       if constexpr (s > 2) __syncthreads();
     };
     if constexpr (S::NS >= 4) stage_inv(ic<4>{});
@@ -567,16 +587,16 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
 
     if constexpr (S::NS > 1)
     {
-      if constexpr (S::CS > 1) cg::this_cluster().sync(); else __syncthreads();
+      if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
     }
 
     // ---------------- inverse stage 1 and store ----------------
     float2 *dstp = a.out + row * a.out_rs;
-    float4 twn[S::H1];
+    float4 tw1[S::H1];
     if constexpr (S::NS > 1)
     {
 #pragma unroll
-      for (int qp = 0; qp < S::H1; ++qp) twn[qp] = ldv4(a.twi + qp * S::D + tr);
+      for (int qp = 0; qp < S::H1; ++qp) tw1[qp] = ldv4(a.twi + qp * S::D + tr);
     }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
@@ -585,14 +605,6 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
       cpair z[S::H1];
       if constexpr (S::NS > 1)
       {
-        float4 twc[S::H1];
-#pragma unroll
-        for (int qp = 0; qp < S::H1; ++qp) twc[qp] = twn[qp];
-        if (g + 1 < S::G1)
-        {
-#pragma unroll
-          for (int qp = 0; qp < S::H1; ++qp) twn[qp] = ldv4(a.twi + qp * S::D + n + S::TPR);
-        }
         float4 v[S::H1];
 #pragma unroll
         for (int qp = 0; qp < S::H1; ++qp)
@@ -601,7 +613,8 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
           v[qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)));
         }
 #pragma unroll
-        for (int qp = 0; qp < S::H1; ++qp) z[qp] = cp_mul4c(cp_from4(v[qp]), twc[qp]);
+        for (int qp = 0; qp < S::H1; ++qp)
+          z[qp] = cp_rot2<+1>(cp_mul4c(cp_from4(v[qp]), tw1[qp]), (g * 2 * qp) & 31, (g * (2 * qp + 1)) & 31);
       }
       else
       {
@@ -628,7 +641,7 @@ __global__ void __launch_bounds__(kThreads, 2) rows_kernel(RowArgs a)
         }
       }
     }
-    if constexpr (S::CS > 1) cg::this_cluster().sync();
+    if constexpr (CL) cg::this_cluster().sync();
   }
 }
 

@@ -18,6 +18,7 @@ SchedRT sched_rt(int logn);
 struct KernelInfo
 {
   const void *fn = nullptr;
+  int threads = 256;     // threads per CTA
   int cluster = 1;       // CTAs per row (thread-block cluster size)
   int rows_per_cta = 1;  // rows per CTA when cluster == 1
   int smem = 0;          // dynamic shared memory per CTA, bytes
@@ -25,6 +26,8 @@ struct KernelInfo
 };
 
 const KernelInfo *kernel_info(int logn, int mode);
+int set_variant(int logn, int mode, int threads);
+int get_variant(int logn, int mode);
 int prepare_kernel(const KernelInfo *k);
 int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaStream_t st);
 

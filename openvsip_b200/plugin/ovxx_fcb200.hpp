@@ -1,0 +1,360 @@
+// OpenVSIP plugin that routes the fast-convolution path to the B200 backend
+// (libfcb200.so, C ABI in include/fcb200.h).  Include it (or pass it with
+// -include) before any code that constructs a vsip::Fftm; link -lfcb200.
+// No reference header is modified: the plugin fills two dispatch slots the
+// reference already reserves.
+//
+//  1. be::user for op::fftm<complex<float>, complex<float>, row, D, R, N>.
+//     be::user is the first entry of List<op::fftm> (src/ovxx/signal/fft.hpp:
+//     57-64), so every row-wise complex<float> vsip::Fftm whose length the
+//     backend supports (powers of two up to 65536) is built on the B200.  The
+//     backend object follows the fftm_backend contract
+//     (src/ovxx/signal/fft/backend.hpp:696-784): it asks the DDA layer for
+//     dense, row-major, interleaved data (anything else is copied by
+//     dda::Rt_data before the call) and applies the scale itself
+//     (supports_scale() == true), so the workspace's separate scale pass
+//     (src/ovxx/signal/fft/workspace.hpp:474-478) is skipped.  Lengths the
+//     backend does not support fail rt_valid() and the dispatcher moves on to
+//     the next backend in the list, exactly as for any other plugin.
+//
+//  2. be::fc_expr for op::assign<2>, the "fused fastconv" slot that the
+//     reference lists (src/ovxx/assign_fwd.hpp:58, src/ovxx/dispatcher/
+//     tags.hpp:33-34) but never implements.  It matches
+//         out = inv_fftm(vmmul<0>(weights, fwd_fftm(in)))     (vector form)
+//         out = inv_fftm(W * fwd_fftm(in)), inv_fftm(fwd_fftm(in) * W)
+//                                                              (matrix form)
+//     when both Fftm objects are B200 ones, and runs the whole expression as
+//     one fused kernel pass (one HBM read and write per sample) instead of
+//     falling through to be::rbo_expr (src/ovxx/assign/rbo.hpp:18-32), which
+//     evaluates the forward FFT into a temporary, copies the vmmul element by
+//     element and runs the inverse and the scale pass.
+//
+// Errors: construction throws (std::runtime_error, or std::bad_alloc when the
+// device is out of memory) like the reference's planners
+// (src/ovxx/fftw/fftw.cpp:97-102).  A failure inside a VSIP_NOTHROW call is
+// raised through OVXX_DO_THROW, as the base-class backends do for
+// unimplemented paths.  A missing GPU is an error at construction, not a
+// silent fall back.
+//
+// Environment: FCB200_DEVICE selects the CUDA device (default 0);
+// FCB200_TRACE=1 prints one line per backend constructed and per fused call.
+#ifndef OVXX_FCB200_HPP
+#define OVXX_FCB200_HPP
+
+#include <vsip/support.hpp>
+#include <vsip/domain.hpp>
+#include <vsip/vector.hpp>
+#include <vsip/matrix.hpp>
+#include <vsip/signal.hpp>
+#include <vsip/math.hpp>
+#include <vsip/dda.hpp>
+#include <ovxx/signal/fft/backend.hpp>
+
+#include <fcb200.h>
+
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace ovxx
+{
+namespace fcb200
+{
+typedef std::complex<float> ctype;
+
+inline bool trace()
+{
+  static bool const t = std::getenv("FCB200_TRACE") != 0;
+  return t;
+}
+
+inline void check(int rc)
+{
+  if (rc == FCB_OK) return;
+  std::string msg = std::string("fcb200: ") + fcb_last_error();
+  if (rc == FCB_ERR_NOMEM) OVXX_DO_THROW(std::bad_alloc());
+  OVXX_DO_THROW(std::runtime_error(msg));
+}
+
+// Select the device once per thread (reference library init is per thread,
+// src/ovxx/library.cpp:36-48).
+inline void ensure_device()
+{
+  static thread_local bool done = false;
+  if (done) return;
+  char const *env = std::getenv("FCB200_DEVICE");
+  check(fcb_init(env ? std::atoi(env) : 0));
+  done = true;
+}
+
+/// fftm_backend for row-wise complex<float> multiple FFTs on the B200.
+template <int D>
+class fftm : public signal::fft::fftm_backend<ctype, ctype, 0, D>
+{
+public:
+  fftm(Domain<2> const &dom, float scale)
+    : rows_(dom[0].size()), cols_(dom[1].size()), scale_(scale), plan_(0), fused_(0), fused_scale_(0.f)
+  {
+    ensure_device();
+    check(fcb_plan_fftm((long long)cols_, (long long)rows_, D == fft_fwd ? FCB_FORWARD : FCB_INVERSE,
+                        scale, &plan_));
+    if (trace())
+      std::fprintf(stderr, "[fcb200] Fftm<%s> %lu x %lu scale %g on the B200\n",
+                   D == fft_fwd ? "fwd" : "inv", (unsigned long)rows_, (unsigned long)cols_, (double)scale);
+  }
+  ~fftm()
+  {
+    if (fused_) fcb_destroy(fused_);
+    if (plan_) fcb_destroy(plan_);
+  }
+  virtual char const *name() { return "fcb200::fftm"; }
+  virtual bool supports_scale() { return true; }
+  virtual void query_layout(Rt_layout<2> &inout)
+  {
+    inout.packing = dense;
+    inout.order = tuple<0, 1, 2>();
+    inout.storage_format = array;
+  }
+  virtual void query_layout(Rt_layout<2> &in, Rt_layout<2> &out)
+  {
+    query_layout(in);
+    out = in;
+  }
+  virtual bool requires_copy(Rt_layout<2> &) { return false; }
+  virtual void in_place(ctype *inout, stride_type r, stride_type c, length_type rows, length_type cols)
+  {
+    run(inout, r, c, inout, r, c, rows, cols);
+  }
+  virtual void out_of_place(ctype *in, stride_type ir, stride_type ic, ctype *out, stride_type o_r,
+                            stride_type oc, length_type rows, length_type cols)
+  {
+    run(in, ir, ic, out, o_r, oc, rows, cols);
+  }
+
+  float scale() const { return scale_; }
+  length_type rows() const { return rows_; }
+  length_type cols() const { return cols_; }
+
+  /// Fused plan for inv(weights .* fwd(x)) * s, cached while the weights
+  /// (already multiplied by s * N) stay the same.  weights: wrows x cols.
+  fcb_plan fused(ctype const *w, stride_type w_rs, length_type wrows, float s, length_type rows_max)
+  {
+    size_t const n = (size_t)(wrows * cols_);
+    bool same = fused_ && fused_rows_ == wrows && fused_scale_ == s && fused_w_.size() == n;
+    for (length_type r = 0; same && r < wrows; ++r)
+      same = std::memcmp(&fused_w_[r * cols_], w + r * w_rs, sizeof(ctype) * cols_) == 0;
+    if (same) return fused_;
+    if (fused_) fcb_destroy(fused_);
+    fused_ = 0;
+    fused_w_.resize(n);
+    std::vector<ctype> scaled(n);
+    for (length_type r = 0; r < wrows; ++r)
+      for (length_type c = 0; c < cols_; ++c)
+      {
+        fused_w_[r * cols_ + c] = w[r * w_rs + c];
+        scaled[r * cols_ + c] = w[r * w_rs + c] * (s * (float)cols_);
+      }
+    check(fcb_plan_fastconv((long long)cols_, (long long)rows_max,
+                            reinterpret_cast<fcb_cf32 const *>(scaled.data()), (long long)wrows,
+                            (long long)cols_, FCB_REPLICA_SPECTRUM, FCB_HOST, &fused_));
+    fused_rows_ = wrows;
+    fused_scale_ = s;
+    return fused_;
+  }
+
+private:
+  void run(ctype *in, stride_type ir, stride_type ic, ctype *out, stride_type o_r, stride_type oc,
+           length_type rows, length_type cols)
+  {
+    OVXX_PRECONDITION(ic == 1 && oc == 1 && cols == cols_);
+    if (rows == 0) return;
+    check(fcb_exec(plan_, reinterpret_cast<fcb_cf32 const *>(in), rows > 1 ? ir : cols,
+                   reinterpret_cast<fcb_cf32 *>(out), rows > 1 ? o_r : cols, (long long)rows, FCB_HOST));
+  }
+
+  length_type rows_, cols_;
+  float scale_;
+  fcb_plan plan_;
+  fcb_plan fused_;
+  std::vector<ctype> fused_w_;
+  length_type fused_rows_ = 0;
+  float fused_scale_;
+};
+
+// Fused plan for a weights block: a vector (one replica spectrum for all rows)
+// or a matrix (one per row), read through the DDA layer (direct pointer when
+// the block is dense, a copy otherwise).
+template <typename W, dimension_type Dim = W::dim> struct fused_plan_for;
+template <typename W> struct fused_plan_for<W, 1>
+{
+  static fcb_plan get(fftm<fft_inv> &g, W const &w, float s, length_type rows)
+  {
+    vsip::dda::Data<W, vsip::dda::in, Layout<1, row1_type, dense, array> > d(w);
+    return g.fused(d.ptr(), g.cols(), 1, s, rows);
+  }
+};
+template <typename W> struct fused_plan_for<W, 2>
+{
+  static fcb_plan get(fftm<fft_inv> &g, W const &w, float s, length_type rows)
+  {
+    vsip::dda::Data<W, vsip::dda::in, Layout<2, row2_type, dense, array> > d(w);
+    return g.fused(d.ptr(), d.size(0) > 1 ? d.stride(0) : g.cols(), d.size(0), s, rows);
+  }
+};
+
+// Run one fused call: in -> out with weights (vector or matrix) on the plans
+// of the two B200 Fftm objects.
+template <typename LHS, typename IN, typename W>
+void run_fused(LHS &lhs, IN const &in_block, W const &w_block, length_type wrows, fftm<fft_fwd> const &f,
+               fftm<fft_inv> &g)
+{
+  typedef Layout<2, row2_type, dense, array> L2;
+  length_type const rows = lhs.size(2, 0), cols = lhs.size(2, 1);
+  vsip::dda::Data<IN, vsip::dda::in, L2> in_data(in_block);
+  vsip::dda::Data<LHS, vsip::dda::out, L2> out_data(lhs);
+  fcb_plan plan = fused_plan_for<W>::get(g, w_block, f.scale() * g.scale(), rows);
+  if (trace())
+    std::fprintf(stderr, "[fcb200] fused fastconv %lu x %lu (%s weights) on the B200\n", (unsigned long)rows,
+                 (unsigned long)cols, wrows == 1 ? "vector" : "matrix");
+  check(fcb_exec(plan, reinterpret_cast<fcb_cf32 const *>(in_data.ptr()), rows > 1 ? in_data.stride(0) : cols,
+                 reinterpret_cast<fcb_cf32 *>(out_data.ptr()), rows > 1 ? out_data.stride(0) : cols,
+                 (long long)rows, FCB_HOST));
+}
+
+template <typename F>
+fftm<fft_fwd> const *as_fwd(F const &functor)
+{
+  return dynamic_cast<fftm<fft_fwd> const *>(&functor.backend());
+}
+template <typename F>
+fftm<fft_inv> *as_inv(F const &functor)
+{
+  return const_cast<fftm<fft_inv> *>(dynamic_cast<fftm<fft_inv> const *>(&functor.backend()));
+}
+
+} // namespace ovxx::fcb200
+
+namespace dispatcher
+{
+
+/// Row-wise complex<float> Fftm on the B200 (be::user slot).
+template <int D, vsip::return_mechanism_type R, unsigned N>
+struct Evaluator<op::fftm<std::complex<float>, std::complex<float>, 0, D, R, N>, be::user,
+                 std::unique_ptr<signal::fft::fftm_backend<std::complex<float>, std::complex<float>, 0, D> >
+                 (Domain<2> const &, float)>
+{
+  typedef signal::fft::fftm_backend<std::complex<float>, std::complex<float>, 0, D> backend_type;
+  static bool const ct_valid = true;
+  static char const *name() { return "fcb200 fftm (B200)"; }
+  static bool rt_valid(Domain<2> const &dom, float)
+  {
+    return fcb_supported_length((long long)dom[1].size()) && dom[0].size() > 0;
+  }
+  static std::unique_ptr<backend_type> exec(Domain<2> const &dom, float scale)
+  {
+    return std::unique_ptr<backend_type>(new fcb200::fftm<D>(dom, scale));
+  }
+};
+
+/// out = inv_fftm(vmmul<0>(weights, fwd_fftm(in))) as one fused pass (be::fc_expr slot).
+template <typename LHS, template <typename> class O1, typename VB, template <typename> class O2, typename MB>
+struct Evaluator<op::assign<2>, be::fc_expr,
+                 void(LHS &, expr::Unary<O1, expr::Vmmul<0, VB, expr::Unary<O2, MB> const> const> const &)>
+{
+  typedef std::complex<float> C;
+  typedef expr::Unary<O2, MB> fwd_block;
+  typedef expr::Vmmul<0, VB, fwd_block const> vmmul_block;
+  typedef expr::Unary<O1, vmmul_block const> RHS;
+  typedef O1<vmmul_block const> inv_functor;
+  typedef O2<MB> fwd_functor;
+  static bool const ct_valid =
+    is_same<typename inv_functor::backend_type, signal::fft::fftm_backend<C, C, 0, fft_inv> >::value &&
+    is_same<typename fwd_functor::backend_type, signal::fft::fftm_backend<C, C, 0, fft_fwd> >::value &&
+    is_same<typename VB::value_type, C>::value && is_same<typename LHS::value_type, C>::value &&
+    is_same<typename MB::value_type, C>::value;
+  static char const *name() { return "fcb200 fused fastconv, vector weights (B200)"; }
+  static bool rt_valid(LHS &, RHS const &rhs)
+  {
+    return fcb200::as_inv(rhs.operation()) && fcb200::as_fwd(rhs.arg().get_mblk().operation());
+  }
+  static void exec(LHS &lhs, RHS const &rhs)
+  {
+    fwd_functor const &f = rhs.arg().get_mblk().operation();
+    fcb200::run_fused(lhs, f.arg(), rhs.arg().get_vblk(), 1, *fcb200::as_fwd(f), *fcb200::as_inv(rhs.operation()));
+  }
+};
+
+/// out = inv_fftm(W * fwd_fftm(in)) and inv_fftm(fwd_fftm(in) * W): one
+/// replica spectrum per row (matrix of coefficients).
+template <typename LHS, template <typename> class O1, template <typename, typename> class M, typename WB,
+          template <typename> class O2, typename MB>
+struct Evaluator<op::assign<2>, be::fc_expr,
+                 void(LHS &, expr::Unary<O1, expr::Binary<M, WB, expr::Unary<O2, MB> const, true> const> const &)>
+{
+  typedef std::complex<float> C;
+  typedef expr::Unary<O2, MB> fwd_block;
+  typedef expr::Binary<M, WB, fwd_block const, true> mul_block;
+  typedef expr::Unary<O1, mul_block const> RHS;
+  typedef O1<mul_block const> inv_functor;
+  typedef O2<MB> fwd_functor;
+  static bool const ct_valid =
+    is_same<M<C, C>, expr::op::Mult<C, C> >::value &&
+    is_same<typename inv_functor::backend_type, signal::fft::fftm_backend<C, C, 0, fft_inv> >::value &&
+    is_same<typename fwd_functor::backend_type, signal::fft::fftm_backend<C, C, 0, fft_fwd> >::value &&
+    is_same<typename WB::value_type, C>::value && is_same<typename LHS::value_type, C>::value &&
+    is_same<typename MB::value_type, C>::value && WB::dim == 2;
+  static char const *name() { return "fcb200 fused fastconv, matrix weights (B200)"; }
+  static bool rt_valid(LHS &lhs, RHS const &rhs)
+  {
+    return fcb200::as_inv(rhs.operation()) && fcb200::as_fwd(rhs.arg().arg2().operation()) &&
+           rhs.arg().arg1().size(2, 0) == lhs.size(2, 0);
+  }
+  static void exec(LHS &lhs, RHS const &rhs)
+  {
+    fwd_functor const &f = rhs.arg().arg2().operation();
+    fcb200::run_fused(lhs, f.arg(), rhs.arg().arg1(), lhs.size(2, 0), *fcb200::as_fwd(f),
+                      *fcb200::as_inv(rhs.operation()));
+  }
+};
+
+template <typename LHS, template <typename> class O1, template <typename, typename> class M, typename WB,
+          template <typename> class O2, typename MB>
+struct Evaluator<op::assign<2>, be::fc_expr,
+                 void(LHS &, expr::Unary<O1, expr::Binary<M, expr::Unary<O2, MB> const, WB, true> const> const &)>
+{
+  typedef std::complex<float> C;
+  typedef expr::Unary<O2, MB> fwd_block;
+  typedef expr::Binary<M, fwd_block const, WB, true> mul_block;
+  typedef expr::Unary<O1, mul_block const> RHS;
+  typedef O1<mul_block const> inv_functor;
+  typedef O2<MB> fwd_functor;
+  static bool const ct_valid =
+    is_same<M<C, C>, expr::op::Mult<C, C> >::value &&
+    is_same<typename inv_functor::backend_type, signal::fft::fftm_backend<C, C, 0, fft_inv> >::value &&
+    is_same<typename fwd_functor::backend_type, signal::fft::fftm_backend<C, C, 0, fft_fwd> >::value &&
+    is_same<typename WB::value_type, C>::value && is_same<typename LHS::value_type, C>::value &&
+    is_same<typename MB::value_type, C>::value && WB::dim == 2;
+  static char const *name() { return "fcb200 fused fastconv, matrix weights (B200)"; }
+  static bool rt_valid(LHS &lhs, RHS const &rhs)
+  {
+    return fcb200::as_inv(rhs.operation()) && fcb200::as_fwd(rhs.arg().arg1().operation()) &&
+           rhs.arg().arg2().size(2, 0) == lhs.size(2, 0);
+  }
+  static void exec(LHS &lhs, RHS const &rhs)
+  {
+    fwd_functor const &f = rhs.arg().arg1().operation();
+    fcb200::run_fused(lhs, f.arg(), rhs.arg().arg2(), lhs.size(2, 0), *fcb200::as_fwd(f),
+                      *fcb200::as_inv(rhs.operation()));
+  }
+};
+
+} // namespace ovxx::dispatcher
+} // namespace ovxx
+
+#endif

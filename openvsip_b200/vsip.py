@@ -101,9 +101,11 @@ class _Plan:
         cl = ctypes.c_int()
         rpc = ctypes.c_int()
         sm = ctypes.c_int()
+        th = ctypes.c_int()
         check(lib().fcb_plan_info(self._handle, ctypes.byref(n), ctypes.byref(cl), ctypes.byref(rpc),
-                                  ctypes.byref(sm)))
-        return {"n": n.value, "cluster_ctas": cl.value, "rows_per_cta": rpc.value, "smem_bytes": sm.value}
+                                  ctypes.byref(sm), ctypes.byref(th)))
+        return {"n": n.value, "cluster_ctas": cl.value, "rows_per_cta": rpc.value, "smem_bytes": sm.value,
+                "threads": th.value}
 
     def _exec(self, inp, out):
         ip, r, c, irs, iw = _desc(inp, False)

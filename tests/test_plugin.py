@@ -1,0 +1,74 @@
+"""The drop-in boundary exercised through the reference's own public API.
+
+openvsip_b200/plugin/_bin holds programs built (where the reference sources
+exist) from the reference's unmodified tests/fastconv.cpp and tests/fftm.cpp
+with the B200 plugin injected (-include ovxx_fcb200.hpp), and plugin_check.cpp,
+which runs the phased, fused and matrix-of-coefficients forms through vsip::Fftm
+/ vmmul on seeded data.  The reference tests self-check (test_assert aborts,
+-100 dB thresholds); FCB200_TRACE shows that the B200 backend, not the
+reference's generic one, ran."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import HAS_GPU, crandn
+
+BIN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "openvsip_b200", "plugin", "_bin")
+
+
+def _prog(name):
+    p = os.path.join(BIN, name)
+    if not os.path.exists(p):
+        pytest.skip(f"{name} not built (needs the reference sources at build time)")
+    return p
+
+
+def _run(args, **kw):
+    env = dict(os.environ, FCB200_TRACE="1")
+    return subprocess.run(args, capture_output=True, text=True, env=env, timeout=600, **kw)
+
+
+@pytest.mark.skipif(HAS_GPU, reason="checks the no-device error path")
+def test_plugin_fails_loudly_without_gpu():
+    r = _run([_prog("fastconv_test")])
+    assert r.returncode != 0
+    assert "fcb200" in r.stderr and "device" in r.stderr
+
+
+@pytest.mark.gpu
+def test_reference_fastconv_test_on_b200():
+    r = _run([_prog("fastconv_test")])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "[fcb200] Fftm<fwd>" in r.stderr
+    assert "[fcb200] fused fastconv" in r.stderr and "vector weights" in r.stderr
+    assert "matrix weights" in r.stderr
+
+
+@pytest.mark.gpu
+def test_reference_fftm_test_on_b200():
+    r = _run([_prog("fftm_test")])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "[fcb200] Fftm<fwd>" in r.stderr and "[fcb200] Fftm<inv>" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,cols", [(64, 4096), (8, 32768)])
+def test_plugin_forms_match_oracle(oracle, tmp_path, rows, cols):
+    rng = np.random.default_rng(rows + cols)
+    x = crandn(rng, (rows, cols))
+    w = crandn(rng, (cols,))
+    x.tofile(tmp_path / "in.bin")
+    w.tofile(tmp_path / "w.bin")
+    r = _run([_prog("plugin_check"), str(rows), str(cols), str(tmp_path / "in.bin"), str(tmp_path / "w.bin"),
+              str(tmp_path / "out")])
+    assert r.returncode == 0, r.stderr[-2000:]
+    want = oracle.fastconv(x, w)
+    for form in ("phased", "fused"):
+        y = np.fromfile(tmp_path / f"out.{form}.bin", dtype=np.complex64).reshape(rows, cols)
+        assert oracle.rel_l2(y, want) <= 2e-6, form
+    wm = (w[None, :] * (1 + np.arange(rows, dtype=np.float32)[:, None] / rows)).astype(np.complex64)
+    ym = np.fromfile(tmp_path / "out.fusedm.bin", dtype=np.complex64).reshape(rows, cols)
+    assert oracle.rel_l2(ym, oracle.fastconv(x, wm)) <= 2e-6
+    assert r.stderr.count("fused fastconv") >= 2
