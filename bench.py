@@ -204,6 +204,42 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_sweep(args):
+    """Per-length throughput of the fused fast convolution and the forward row
+    Fftm (the 256 x {256..65536} sweep shape, and a fixed 2^24-sample batch per
+    length), one JSON line per (kind, length); kernel time by CUDA events."""
+    import torch
+
+    import openvsip_b200 as ov
+    torch.cuda.set_device(0)
+    peak, _ = measured_peak()
+    stream = torch.cuda.current_stream()
+    for logn in range(8, 17):
+        n = 1 << logn
+        for rows_label, rows in (("256 rows", 256), ("2^24 samples", (1 << 24) // n)):
+            x = (torch.randn(rows, n, dtype=torch.complex64, device="cuda"))
+            y = torch.empty_like(x)
+            rep = np.ones(n, dtype=np.complex64)
+            for kind, plan in (("fastconv", ov.Fastconv(rep, rows)), ("fftm_fwd", ov.Fftm(rows, n, ov.fft_fwd))):
+                if args.threads:
+                    pass
+                for _ in range(3):
+                    plan(x, y)
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                ev[0].record(stream)
+                for _ in range(args.steps):
+                    plan(x, y)
+                ev[1].record(stream)
+                torch.cuda.synchronize()
+                ms = ev[0].elapsed_time(ev[1]) / args.steps
+                alg = 16.0 * rows * n + (8.0 * n if kind == "fastconv" else 0.0)
+                gbs = alg / (ms / 1e3) / 1e9
+                print(json.dumps({"sweep": kind, "n": n, "rows": rows, "shape": rows_label, "ms": ms,
+                                  "samples_per_s": rows * n / (ms / 1e3), "gbs": gbs, "frac": gbs / peak,
+                                  "threads": plan.info()["threads"], "cluster": plan.info()["cluster_ctas"]}),
+                      flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -213,9 +249,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--threads", type=int, default=0, help="force the 256- or 512-thread kernel variant")
+    ap.add_argument("--sweep", action="store_true", help="per-length throughput lines instead of the benchmark")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
+    if args.sweep:
+        run_sweep(args)
+        return
 
     if args.impl == "reference":
         run_reference(args, world, rank)
