@@ -250,6 +250,13 @@ int prepare_kernel(const KernelInfo *k)
   // Idempotent; cheap after the first call per device.
   cudaError_t e = cudaFuncSetAttribute(k->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k->smem);
   if (e != cudaSuccess) return cuda_error(e, "cudaFuncSetAttribute(smem)");
+  // tiles resident at once: the L2 prefetch distance
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k->fn, k->threads, k->smem);
+  if (e != cudaSuccess) return cuda_error(e, "occupancy query");
+  const_cast<KernelInfo *>(k)->resident_tiles = (long long)sms * (per_sm > 0 ? per_sm : 1) / k->cluster;
   return FCB_OK;
 }
 
@@ -273,7 +280,9 @@ int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaSt
     cfg.attrs = attr;
     cfg.numAttrs = 1;
   }
-  void *params[] = {const_cast<RowArgs *>(&args)};
+  RowArgs a = args;
+  if (a.ahead < 0) a.ahead = k->resident_tiles;  // one resident wave of tiles ahead
+  void *params[] = {&a};
   cudaError_t e = cudaLaunchKernelExC(&cfg, k->fn, params);
   if (e != cudaSuccess) return cuda_error(e, "row kernel launch");
   return FCB_OK;

@@ -310,7 +310,15 @@ struct RowArgs
   const float4 *rep;    // fused: replica pair table (slot order, scaled 1/N)
   long long rep_rs;     // fused: replica row stride in slots (0 = one vector)
   float scale;          // standalone: output scale
+  long long ahead;      // L2 prefetch distance in tiles (CTAs, or clusters) -- about
+                        // one resident wave, so that tile's rows stream from HBM
+                        // into L2 while this tile computes; 0 = off
 };
+
+__device__ __forceinline__ void prefetch_l2(const void *p)
+{
+  asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
 
 enum Mode { kFwd = 0, kInv = 1, kFastconv = 2 };
 
@@ -367,6 +375,22 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
     float4 *dst = reinterpret_cast<float4 *>(smem + S::SLOTS);
 #pragma unroll 4
     for (int i = t; i < S::TWS / 2; i += THREADS) dst[i] = __ldg(src + i);
+  }
+
+  // prefetch into L2 the input of the tile that runs about one wave later
+  if (a.ahead > 0)
+  {
+    const long long tile = CL ? (long long)(blockIdx.x / S::CS) : (long long)blockIdx.x;
+    const long long row0 = (tile + a.ahead) * S::ROWS;
+    constexpr int LPR = S::N >= 16 ? S::N / 16 : 1;          // 128-byte lines per row
+    constexpr int LINES = S::ROWS * LPR / S::CS;             // lines of this CTA's part
+#pragma unroll 1
+    for (int i = t; i < LINES; i += THREADS)
+    {
+      const int li = rank * LINES + i;
+      const long long r = row0 + li / LPR;
+      if (r < a.rows) prefetch_l2(a.in + r * a.in_rs + (long long)(li % LPR) * 16);
+    }
   }
 
   cpair c[S::CPT];

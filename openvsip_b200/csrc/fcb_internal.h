@@ -23,6 +23,7 @@ struct KernelInfo
   int rows_per_cta = 1;  // rows per CTA when cluster == 1
   int smem = 0;          // dynamic shared memory per CTA, bytes
   long long tw_bytes = 0; // twiddle table size
+  long long resident_tiles = 0;  // CTAs (or clusters) resident at once, set by prepare_kernel
 };
 
 const KernelInfo *kernel_info(int logn, int mode);
