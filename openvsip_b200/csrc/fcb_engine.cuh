@@ -336,6 +336,23 @@ struct SlotMap
 template <int S_>
 using ic = std::integral_constant<int, S_>;
 
+// Barrier over the NT consecutive threads that share one exchange (NT a power
+// of two dividing THREADS): a warp barrier when they sit in one warp, a named
+// barrier per group otherwise, the CTA barrier when the group is the CTA.
+// Between stage s and s+1 only the St(s) = L(s)/16 threads that own one block
+// of L(s) slots exchange data, so narrower barriers let the groups of a CTA
+// run out of phase (one group's shared-memory traffic overlaps another's math).
+template <int NT, int THREADS>
+__device__ __forceinline__ void group_sync(int t)
+{
+  if constexpr (NT <= 32)
+    __syncwarp();
+  else if constexpr (NT >= THREADS)
+    __syncthreads();
+  else
+    asm volatile("bar.sync %0, %1;" :: "r"(1 + t / NT), "r"(NT) : "memory");
+}
+
 template <int LOGN, int MODE, int THREADS>
 __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
 {
@@ -497,7 +514,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
 #pragma unroll
       for (int i = 0; i < 16; ++i)
         st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, 4), rho)), cp_to4(c[i]));
-      __syncthreads();
+      group_sync<St, THREADS>(t);  // stage s+1 reads only this block of Lg slots
     }
   };
   if constexpr (S::NS >= 2) stage_fwd(ic<2>{});
@@ -603,7 +620,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
 #pragma unroll
       for (int i = 0; i < 16; ++i)
         st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, 4), rho)), cp_to4(z[i]));
-      if constexpr (s > 2) __syncthreads();
+      if constexpr (s > 2) group_sync<S::S(s - 1), THREADS>(t);  // stage s-1 reads blocks of L(s-1)
     };
     if constexpr (S::NS >= 4) stage_inv(ic<4>{});
     if constexpr (S::NS >= 3) stage_inv(ic<3>{});
