@@ -143,6 +143,19 @@ FCB_API int fcb_vmmul_rows(const fcb_cf32 *v, const fcb_cf32 *m, long long m_rs,
 FCB_API int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int matched,
                          fcb_cf32 *spectrum_dev);
 
+/* The same replica spectrum for callers that must not allocate device memory
+ * while running (for example a real-time pulse-compression loop with a fixed
+ * memory budget, or a process whose device memory is reserved up front).  No
+ * counterpart in the reference.  Its FP64 work buffers are a 2 MiB array built
+ * into the library (held on every GPU that loads it until exit) instead of a
+ * per-call allocation, so n is limited to 65536; larger n is rejected with
+ * FCB_ERR_INVALID.  Asynchronous on `stream` (NULL: the default stream); it
+ * calls no allocator.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+FCB_API int fcb_replica_spectrum_noalloc(const fcb_cf32 *replica_dev, long long n, int matched,
+                                         fcb_cf32 *spectrum_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

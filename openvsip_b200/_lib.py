@@ -73,6 +73,7 @@ SIGNATURES = {
     "fcb_tune_get": (c_int, [c_ll, c_int]),
     "fcb_vmmul_rows": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_ll, c_vp]),
     "fcb_replica_spectrum": (c_int, [c_vp, c_ll, c_int, c_vp]),
+    "fcb_replica_spectrum_noalloc": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp]),
     "fcb_batch_create": (c_int, [c_ll, c_ll, ctypes.POINTER(c_vp)]),
     "fcb_batch_add_replica": (c_int, [c_vp, c_vp, c_ll, c_int, c_int, ctypes.POINTER(c_int)]),
     "fcb_batch_run": (c_int, [c_vp, c_vp, c_int, c_int]),

@@ -352,3 +352,69 @@ int launch_scale_rows(const float2 *in, long long in_rs, float2 *out, long long 
 }
 
 }  // namespace fcb
+
+// ---------------------------------------------------------------------------
+// Replica spectrum without any allocation.
+//
+// Some callers cannot allocate device memory once they are running: a
+// real-time pulse-compression loop that must not stall in the allocator or
+// fail on a fragmented heap mid-mission, a process whose device memory is
+// fully reserved up front, or code that runs while another component owns
+// the allocator.  fcb_replica_spectrum_noalloc computes the same FP64 replica
+// spectrum as fcb_replica_spectrum, but its two FP64 ping-pong buffers live in
+// the file-scope array below instead of a per-call cudaMallocAsync.
+//
+// The array is 2 * 65536 double2 = 2 MiB; every GPU that loads this library
+// holds it until the process exits.  Calls share it and it keeps the last
+// call's contents; nothing in it needs to start at zero (each call writes a
+// buffer completely before reading it).  Calls that overlap on the GPU (on
+// different streams, or from different threads) race on it.
+namespace {
+constexpr long long kNoAllocMaxN = 65536;
+__device__ __align__(256) double2 g_noalloc_scratch[2 * kNoAllocMaxN];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double2 *g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  The first call
+// on each device looks it up with cudaGetSymbolAddress (host code cannot use
+// the array's name as a device address).
+int noalloc_scratch(double2 **out)
+{
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fcb::cuda_error(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fcb::set_error(FCB_ERR_UNSUPPORTED, "device index %d too large", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev])
+  {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return fcb::cuda_error(e, "cudaGetSymbolAddress(scratch)");
+    g_noalloc_ptr[dev] = static_cast<double2 *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return FCB_OK;
+}
+}  // namespace
+
+extern "C" FCB_API int fcb_replica_spectrum_noalloc(const fcb_cf32 *replica_dev, long long n, int matched,
+                                                    fcb_cf32 *spectrum_dev, void *stream)
+{
+  if (n < 1 || (n & (n - 1)) != 0)
+    return fcb::set_error(FCB_ERR_UNSUPPORTED, "length %lld is not a power of two", n);
+  if (n > kNoAllocMaxN)
+    return fcb::set_error(FCB_ERR_INVALID, "length %lld exceeds the no-allocation scratch limit of %lld samples",
+                          n, kNoAllocMaxN);
+  if (!replica_dev || !spectrum_dev) return fcb::set_error(FCB_ERR_INVALID, "NULL pointer");
+  double2 *scratch = nullptr;
+  int rc = noalloc_scratch(&scratch);
+  if (rc) return rc;
+  fcb::fft_fp64_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float2 *>(replica_dev),
+                                                             scratch, scratch + n, n, matched,
+                                                             reinterpret_cast<float2 *>(spectrum_dev));
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fcb::cuda_error(e, "replica FFT (no allocation)");
+  return FCB_OK;
+}
