@@ -156,6 +156,42 @@ FCB_API int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int m
 FCB_API int fcb_replica_spectrum_noalloc(const fcb_cf32 *replica_dev, long long n, int matched,
                                          fcb_cf32 *spectrum_dev, void *stream);
 
+/* ---- Batched fast convolution ------------------------------------------
+ * Many pulse-compression jobs of uneven shapes (rows x samples, each with its
+ * own replica) run in ONE persistent kernel launch, replayed from a CUDA graph
+ * (the graph resets the kernel's work counter and launches it).  No single
+ * reference counterpart: the reference runs each job's Fftm -> vmmul -> Fftm
+ * (benchmarks/fastconv.cpp:100-106) separately.  Device pointers only; row
+ * lengths are powers of two from 256 to 32768. */
+typedef struct fcb_batch_s *fcb_batch;
+typedef struct
+{
+  const fcb_cf32 *in;   /* device, pulses x n, row stride in_rs */
+  long long in_rs;
+  fcb_cf32 *out;        /* device, may equal in (in place) */
+  long long out_rs;
+  long long pulses;     /* rows */
+  long long n;          /* samples per row */
+  int replica;          /* id from fcb_batch_add_replica (its length must be n) */
+} fcb_job;
+
+/* threads: 256 or 512 threads per CTA, 0 for the default (tuned) variant. */
+FCB_API int fcb_batch_create(int threads, fcb_batch *batch);
+/* Keep a replica resident on the device (spectrum built in FP64 for the time
+ * kinds); returns its id. */
+FCB_API int fcb_batch_add_replica(fcb_batch batch, const fcb_cf32 *replica, long long n,
+                                  int replica_kind, int where, int *id);
+/* Define the job list (copied).  order 0: longest rows first (default load
+ * balance), 1: as given.  Builds the job table and captures the graph. */
+FCB_API int fcb_batch_set_jobs(fcb_batch batch, const fcb_job *jobs, int njobs, int order);
+/* Run all jobs once: one graph launch on the batch's stream (asynchronous). */
+FCB_API int fcb_batch_run(fcb_batch batch);
+FCB_API int fcb_batch_set_stream(fcb_batch batch, void *stream);
+FCB_API int fcb_batch_sync(fcb_batch batch);
+FCB_API int fcb_batch_info(fcb_batch batch, long long *units, long long *samples, int *grid,
+                           int *threads);
+FCB_API int fcb_batch_destroy(fcb_batch batch);
+
 #ifdef __cplusplus
 }
 #endif

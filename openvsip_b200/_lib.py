@@ -74,14 +74,22 @@ SIGNATURES = {
     "fcb_vmmul_rows": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_ll, c_vp]),
     "fcb_replica_spectrum": (c_int, [c_vp, c_ll, c_int, c_vp]),
     "fcb_replica_spectrum_noalloc": (c_int, [c_vp, c_ll, c_int, c_vp, c_vp]),
-    "fcb_batch_create": (c_int, [c_ll, c_ll, ctypes.POINTER(c_vp)]),
+    "fcb_batch_create": (c_int, [c_int, ctypes.POINTER(c_vp)]),
     "fcb_batch_add_replica": (c_int, [c_vp, c_vp, c_ll, c_int, c_int, ctypes.POINTER(c_int)]),
-    "fcb_batch_run": (c_int, [c_vp, c_vp, c_int, c_int]),
+    "fcb_batch_set_jobs": (c_int, [c_vp, c_vp, c_int, c_int]),
+    "fcb_batch_run": (c_int, [c_vp]),
     "fcb_batch_set_stream": (c_int, [c_vp, c_vp]),
     "fcb_batch_sync": (c_int, [c_vp]),
-    "fcb_batch_info": (c_int, [c_vp, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), ctypes.POINTER(c_int)]),
+    "fcb_batch_info": (c_int, [c_vp, ctypes.POINTER(c_ll), ctypes.POINTER(c_ll), ctypes.POINTER(c_int),
+                               ctypes.POINTER(c_int)]),
     "fcb_batch_destroy": (c_int, [c_vp]),
 }
+
+
+class FcbJob(ctypes.Structure):
+    """fcb_job (include/fcb200.h)."""
+    _fields_ = [("in_", c_vp), ("in_rs", c_ll), ("out", c_vp), ("out_rs", c_ll), ("pulses", c_ll),
+                ("n", c_ll), ("replica", c_int)]
 
 
 def header_symbols() -> list[str]:

@@ -1,0 +1,446 @@
+// Batched fast convolution: many pulse-compression jobs of uneven shapes
+// (pulses x samples, each with its own replica) in ONE persistent launch,
+// replayed from a CUDA graph.
+//
+// There is no single counterpart in the reference: there each job is its own
+// Fftm -> vmmul -> Fftm sequence (benchmarks/fastconv.cpp:100-106), run one
+// after another on the host.
+//
+// Work decomposition: a job of P rows of N samples is cut into "units".  A unit
+// is the work of one hardware cluster of CSMAX CTAs for one step: CSMAX row
+// tiles when a row fits in one CTA, or CSMAX/CS rows when CS CTAs share a row.
+// Units of all jobs form one index space (jobs ordered longest rows first by
+// default); each cluster takes the next unit from a global ticket counter (the
+// only scratch memory, reset by a memset node of the same graph) until the
+// space is exhausted, so uneven jobs balance across the GPU.
+#include "fcb200.h"
+#include "fcb_engine.cuh"
+#include "fcb_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <numeric>
+#include <vector>
+
+namespace fcb {
+
+struct BatchJob
+{
+  RowArgs args;
+  int logn;
+  int tiles_per_unit;
+  long long unit_begin;
+};
+
+constexpr int kBatchMinLog = 8;   // 256 samples
+constexpr int kBatchMaxLog = 15;  // 32768 samples
+
+__device__ __forceinline__ long long ld_cluster_s64(uint32_t addr)
+{
+  long long v;
+  asm volatile("ld.shared::cluster.s64 %0, [%1];" : "=l"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+template <int T, int CSMAX>
+__global__ void __launch_bounds__(T, 512 / T)
+    batch_kernel(const BatchJob *__restrict__ jobs, int njobs, long long total_units, unsigned long long *ticket)
+{
+  __shared__ long long s_unit[2];
+  constexpr bool HC = CSMAX > 1;
+  const int hw_rank = HC ? (int)cg::this_cluster().block_rank() : 0;
+  int cur_logn = -1;
+#pragma unroll 1
+  for (int it = 0;; ++it)
+  {
+    // one ticket per cluster, broadcast from rank 0 (double-buffered by parity:
+    // slot it&1 is rewritten only after every CTA passed the next barrier)
+    if (hw_rank == 0 && threadIdx.x == 0) s_unit[it & 1] = (long long)atomicAdd(ticket, 1ULL);
+    long long u;
+    if constexpr (HC)
+    {
+      cg::this_cluster().sync();
+      u = ld_cluster_s64(cluster_addr(smem_addr(&s_unit[it & 1]), 0));
+    }
+    else
+    {
+      __syncthreads();
+      u = s_unit[it & 1];
+    }
+    if (u >= total_units)
+    {
+      if constexpr (HC) cg::this_cluster().sync();  // rank 0 stays until every CTA has read
+      break;
+    }
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi)
+    {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].unit_begin <= u) lo = mid; else hi = mid - 1;
+    }
+    const BatchJob &J = jobs[lo];
+    const long long lu = u - J.unit_begin;
+    const bool copy = J.logn != cur_logn;
+    cur_logn = J.logn;
+    switch (J.logn)
+    {
+#define FCB_BATCH_CASE(L)                                                                    \
+  case L:                                                                                    \
+  {                                                                                          \
+    constexpr int CS = Sched<L, T>::CS;                                                      \
+    static_assert(CS <= CSMAX, "row longer than the launch's cluster");                      \
+    const int sub = hw_rank / CS;                                                            \
+    row_tile<L, kFastconv, T>(J.args, lu * J.tiles_per_unit + sub, hw_rank % CS, sub * CS, copy); \
+  }                                                                                          \
+  break;
+      FCB_BATCH_CASE(8)
+      FCB_BATCH_CASE(9)
+      FCB_BATCH_CASE(10)
+      FCB_BATCH_CASE(11)
+      FCB_BATCH_CASE(12)
+      FCB_BATCH_CASE(13)
+      FCB_BATCH_CASE(14)
+      FCB_BATCH_CASE(15)
+#undef FCB_BATCH_CASE
+      default:
+        break;
+    }
+  }
+}
+
+// Largest shared-memory footprint over the lengths a batch kernel handles.
+template <int T, int L = kBatchMinLog>
+constexpr int batch_smem()
+{
+  if constexpr (L > kBatchMaxLog)
+    return 0;
+  else
+  {
+    constexpr int a = Sched<L, T>::SMEM, b = batch_smem<T, L + 1>();
+    return a > b ? a : b;
+  }
+}
+
+struct BatchVariant
+{
+  const void *fn;
+  int threads, csmax, smem;
+};
+
+static BatchVariant batch_variant(int threads)
+{
+  if (threads == 256)
+    return {(const void *)&batch_kernel<256, Sched<kBatchMaxLog, 256>::CS>, 256, Sched<kBatchMaxLog, 256>::CS,
+            batch_smem<256>()};
+  return {(const void *)&batch_kernel<512, Sched<kBatchMaxLog, 512>::CS>, 512, Sched<kBatchMaxLog, 512>::CS,
+          batch_smem<512>()};
+}
+
+}  // namespace fcb
+
+using namespace fcb;
+
+struct fcb_batch_s
+{
+  int device = 0;
+  BatchVariant v{};
+  int grid = 0;
+  int ctas_per_sm = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  float4 *tw[kMaxLogN + 1] = {};
+  struct Replica { float4 *table; int logn; };
+  std::vector<Replica> replicas;
+  BatchJob *d_jobs = nullptr;
+  int njobs = 0;
+  long long total_units = 0;
+  long long total_samples = 0;
+  unsigned long long *d_ticket = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+int ilog2_exact(long long n)
+{
+  if (n < 1 || (n & (n - 1)) != 0) return -1;
+  int l = 0;
+  while ((1LL << l) < n) ++l;
+  return l;
+}
+
+void drop_graph(fcb_batch b)
+{
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+void batch_free(fcb_batch b)
+{
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->own_stream) cudaStreamSynchronize(b->own_stream);
+  if (b->stream && b->stream != b->own_stream) cudaStreamSynchronize(b->stream);
+  drop_graph(b);
+  for (auto &r : b->replicas) cudaFree(r.table);
+  for (auto *t : b->tw) cudaFree(t);
+  cudaFree(b->d_jobs);
+  cudaFree(b->d_ticket);
+  if (b->own_stream) cudaStreamDestroy(b->own_stream);
+  delete b;
+}
+
+int launch_batch(fcb_batch b, cudaStream_t st)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)b->grid);
+  cfg.blockDim = dim3(b->v.threads);
+  cfg.dynamicSmemBytes = b->v.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  if (b->v.csmax > 1)
+  {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = b->v.csmax;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  const BatchJob *jobs = b->d_jobs;
+  int njobs = b->njobs;
+  long long total = b->total_units;
+  unsigned long long *ticket = b->d_ticket;
+  void *params[] = {&jobs, &njobs, &total, &ticket};
+  cudaError_t e = cudaLaunchKernelExC(&cfg, b->v.fn, params);
+  if (e != cudaSuccess) return cuda_error(e, "batch kernel launch");
+  return FCB_OK;
+}
+
+// Capture "reset the ticket, run the persistent kernel" into a CUDA graph.
+int build_graph(fcb_batch b)
+{
+  drop_graph(b);
+  cudaError_t e = cudaStreamBeginCapture(b->own_stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_error(e, "graph capture");
+  e = cudaMemsetAsync(b->d_ticket, 0, sizeof(unsigned long long), b->own_stream);
+  int rc = e == cudaSuccess ? launch_batch(b, b->own_stream) : cuda_error(e, "ticket reset");
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(b->own_stream, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e2 != cudaSuccess) return cuda_error(e2, "graph capture");
+  b->graph = g;
+  e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (e != cudaSuccess) { drop_graph(b); return cuda_error(e, "graph instantiate"); }
+  return FCB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fcb_batch_create(int threads, fcb_batch *out)
+{
+  if (!out) return set_error(FCB_ERR_INVALID, "batch pointer is NULL");
+  *out = nullptr;
+  if (threads == 0) threads = 512;
+  if (threads != 256 && threads != 512) return set_error(FCB_ERR_INVALID, "threads must be 0, 256 or 512");
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return set_error(FCB_ERR_NODEVICE, "no CUDA device");
+  fcb_batch b = new (std::nothrow) fcb_batch_s;
+  if (!b) return set_error(FCB_ERR_NOMEM, "batch allocation");
+  cudaGetDevice(&b->device);
+  b->v = batch_variant(threads);
+  cudaError_t e = cudaFuncSetAttribute(b->v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, b->v.smem);
+  int rc = e == cudaSuccess ? FCB_OK : cuda_error(e, "batch kernel attributes");
+  if (!rc)
+  {
+    // persistent grid: as many CTAs (whole clusters) as can be resident at once
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->ctas_per_sm, b->v.fn, b->v.threads, b->v.smem);
+    if (e != cudaSuccess || b->ctas_per_sm < 1) rc = cuda_error(e, "batch occupancy");
+    else if (b->v.csmax > 1)
+    {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(sms * b->ctas_per_sm));
+      cfg.blockDim = dim3(b->v.threads);
+      cfg.dynamicSmemBytes = b->v.smem;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = b->v.csmax;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      int clusters = 0;
+      e = cudaOccupancyMaxActiveClusters(&clusters, b->v.fn, &cfg);
+      if (e != cudaSuccess || clusters < 1) rc = cuda_error(e, "batch cluster occupancy");
+      else b->grid = clusters * b->v.csmax;
+    }
+    else
+      b->grid = sms * b->ctas_per_sm;
+  }
+  if (!rc && (e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    rc = cuda_error(e, "cudaStreamCreate");
+  b->stream = b->own_stream;
+  if (!rc && (e = cudaMalloc(&b->d_ticket, sizeof(unsigned long long))) != cudaSuccess)
+    rc = set_error(FCB_ERR_NOMEM, "ticket counter: %s", cudaGetErrorString(e));
+  if (rc) { batch_free(b); return rc; }
+  *out = b;
+  return FCB_OK;
+}
+
+int fcb_batch_add_replica(fcb_batch b, const fcb_cf32 *replica, long long n, int kind, int where, int *id)
+{
+  if (!b || !replica || !id) return set_error(FCB_ERR_INVALID, "NULL argument");
+  const int l = ilog2_exact(n);
+  if (l < kBatchMinLog || l > kBatchMaxLog)
+    return set_error(FCB_ERR_UNSUPPORTED, "batch rows must be powers of two in [%d, %d], got %lld", 1 << kBatchMinLog,
+                     1 << kBatchMaxLog, n);
+  if (kind < FCB_REPLICA_SPECTRUM || kind > FCB_REPLICA_TIME_MATCHED) return set_error(FCB_ERR_INVALID, "bad replica kind");
+  if (where != FCB_HOST && where != FCB_DEVICE) return set_error(FCB_ERR_INVALID, "bad location");
+  cudaSetDevice(b->device);
+  float2 *spec = nullptr, *tmp = nullptr;
+  float4 *table = nullptr;
+  const size_t bytes = sizeof(float2) * (size_t)n;
+  cudaError_t e = cudaMalloc(&spec, bytes);
+  int rc = e == cudaSuccess ? FCB_OK : set_error(FCB_ERR_NOMEM, "replica buffer");
+  if (!rc && (e = cudaMemcpyAsync(spec, replica, bytes, where == FCB_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                                  b->own_stream)) != cudaSuccess)
+    rc = cuda_error(e, "replica copy");
+  if (!rc && kind != FCB_REPLICA_SPECTRUM)
+  {
+    if ((e = cudaMalloc(&tmp, bytes)) != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "replica buffer");
+    if (!rc) rc = replica_spectrum_dev(spec, n, kind == FCB_REPLICA_TIME_MATCHED, tmp, b->own_stream);
+    if (!rc) std::swap(spec, tmp);
+  }
+  if (!rc && (e = cudaMalloc(&table, sizeof(float4) * (size_t)(n / 2))) != cudaSuccess)
+    rc = set_error(FCB_ERR_NOMEM, "replica table");
+  if (!rc) rc = build_replica_table(l, spec, n, 1, table, b->own_stream);
+  if (!rc && !b->tw[l]) rc = build_twiddles(l, &b->tw[l], b->own_stream);
+  if (!rc && (e = cudaStreamSynchronize(b->own_stream)) != cudaSuccess) rc = cuda_error(e, "replica preparation");
+  cudaFree(spec);
+  cudaFree(tmp);
+  if (rc) { cudaFree(table); return rc; }
+  b->replicas.push_back({table, l});
+  *id = (int)b->replicas.size() - 1;
+  return FCB_OK;
+}
+
+int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
+{
+  if (!b || (njobs > 0 && !jobs) || njobs < 0) return set_error(FCB_ERR_INVALID, "bad job list");
+  std::vector<BatchJob> hj;
+  std::vector<int> idx(njobs);
+  std::iota(idx.begin(), idx.end(), 0);
+  for (int i = 0; i < njobs; ++i)
+  {
+    const fcb_job &j = jobs[i];
+    if (j.replica < 0 || j.replica >= (int)b->replicas.size()) return set_error(FCB_ERR_INVALID, "job %d: bad replica id", i);
+    if ((1LL << b->replicas[j.replica].logn) != j.n) return set_error(FCB_ERR_INVALID, "job %d: replica length != row length", i);
+    if (j.pulses < 0 || (j.pulses > 0 && (!j.in || !j.out))) return set_error(FCB_ERR_INVALID, "job %d: bad buffers", i);
+    if (j.in_rs < j.n || j.out_rs < j.n) return set_error(FCB_ERR_INVALID, "job %d: row stride < row length", i);
+  }
+  if (order == 0)  // longest rows first, then most rows: large units start early
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) {
+      return jobs[a].n != jobs[c].n ? jobs[a].n > jobs[c].n : jobs[a].pulses > jobs[c].pulses;
+    });
+  long long units = 0, samples = 0;
+  for (int i : idx)
+  {
+    const fcb_job &j = jobs[i];
+    if (j.pulses == 0) continue;
+    const int l = b->replicas[j.replica].logn;
+    BatchJob bj;
+    bj.logn = l;
+    // geometry of this length on the variant's CTAs (as in Sched<>)
+    const int T = b->v.threads;
+    const int half = (int)(j.n / 2);
+    const int spc = T * 16;
+    const int cs = half > spc ? half / spc : 1;
+    const int rows_per_tile = cs > 1 ? 1 : (T * 32) / (int)j.n;
+    bj.tiles_per_unit = b->v.csmax / cs;
+    const long long rows_per_unit = (long long)bj.tiles_per_unit * rows_per_tile;
+    bj.unit_begin = units;
+    units += (j.pulses + rows_per_unit - 1) / rows_per_unit;
+    samples += j.pulses * j.n;
+    RowArgs &a = bj.args;
+    a.in = reinterpret_cast<const float2 *>(j.in);
+    a.in_rs = j.in_rs;
+    a.out = reinterpret_cast<float2 *>(j.out);
+    a.out_rs = j.out_rs;
+    a.rows = j.pulses;
+    a.tw = b->tw[l];
+    a.twi = b->tw[l];
+    a.rep = b->replicas[j.replica].table;
+    a.rep_rs = 0;
+    a.scale = 1.f;
+    a.ahead = 0;
+    hj.push_back(bj);
+  }
+  cudaSetDevice(b->device);
+  cudaStreamSynchronize(b->stream);
+  drop_graph(b);
+  cudaFree(b->d_jobs);
+  b->d_jobs = nullptr;
+  b->njobs = (int)hj.size();
+  b->total_units = units;
+  b->total_samples = samples;
+  if (hj.empty()) return FCB_OK;
+  cudaError_t e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * hj.size());
+  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "job table");
+  e = cudaMemcpy(b->d_jobs, hj.data(), sizeof(BatchJob) * hj.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_error(e, "job table copy");
+  return build_graph(b);
+}
+
+int fcb_batch_run(fcb_batch b)
+{
+  if (!b) return set_error(FCB_ERR_INVALID, "batch is NULL");
+  if (b->njobs == 0) return FCB_OK;
+  if (!b->exec) return set_error(FCB_ERR_INVALID, "no jobs set");
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+  if (e != cudaSuccess) return cuda_error(e, "graph launch");
+  return FCB_OK;
+}
+
+int fcb_batch_set_stream(fcb_batch b, void *stream)
+{
+  if (!b) return set_error(FCB_ERR_INVALID, "batch is NULL");
+  b->stream = (cudaStream_t)stream;
+  return FCB_OK;
+}
+
+int fcb_batch_sync(fcb_batch b)
+{
+  if (!b) return set_error(FCB_ERR_INVALID, "batch is NULL");
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return cuda_error(e, "batch");
+  return FCB_OK;
+}
+
+int fcb_batch_info(fcb_batch b, long long *units, long long *samples, int *grid, int *threads)
+{
+  if (!b) return set_error(FCB_ERR_INVALID, "batch is NULL");
+  if (units) *units = b->total_units;
+  if (samples) *samples = b->total_samples;
+  if (grid) *grid = b->grid;
+  if (threads) *threads = b->v.threads;
+  return FCB_OK;
+}
+
+int fcb_batch_destroy(fcb_batch b)
+{
+  batch_free(b);
+  return FCB_OK;
+}
+
+}  // extern "C"

@@ -353,8 +353,15 @@ __device__ __forceinline__ void group_sync(int t)
     asm volatile("bar.sync %0, %1;" :: "r"(1 + t / NT), "r"(NT) : "memory");
 }
 
+// One tile of a row transform on this CTA: the ROWS rows of `tile` when a row
+// fits in one CTA, or part `rank` of row `tile` when CS CTAs share a row (they
+// are the cluster ranks rank_base .. rank_base + CS - 1).  copy_tw: load the
+// later-stage twiddle tables into shared memory (a persistent caller skips it
+// while consecutive tiles have the same length).  The caller guarantees that
+// no thread of the CTA (or of the CS CTAs) still reads the slot array of a
+// previous tile.
 template <int LOGN, int MODE, int THREADS>
-__global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
+__device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int rank, int rank_base, bool copy_tw)
 {
   using S = Sched<LOGN, THREADS>;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
@@ -364,11 +371,9 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
   const float2 *tw2 = reinterpret_cast<const float2 *>(a.tw + S::HALF);
 
   const int t = threadIdx.x;
-  int rank = 0;
-  if constexpr (CL) rank = (int)cg::this_cluster().block_rank();
   const int rho = CL ? 0 : t / S::TPR;                       // row within CTA
   const int tr = CL ? rank * THREADS + t : t % S::TPR;       // thread within row
-  const long long row = CL ? (long long)(blockIdx.x / S::CS) : (long long)blockIdx.x * S::ROWS + rho;
+  const long long row = CL ? tile : tile * S::ROWS + rho;
   const bool active = row < a.rows;
 
   // 32-bit base address of every cluster rank's slot array (own array when CS == 1)
@@ -378,7 +383,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
   {
     const uint32_t own = peer[0];
 #pragma unroll
-    for (int r = 0; r < S::CS; ++r) peer[r] = cluster_addr(own, r);
+    for (int r = 0; r < S::CS; ++r) peer[r] = cluster_addr(own, rank_base + r);
   }
   const uint32_t slot_base = smem_addr(smem);
   const uint32_t tw_base = slot_base + 16u * S::SLOTS;  // later-stage twiddles in shared memory
@@ -386,7 +391,7 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
 
   // copy the twiddle tables of stages 2..NS-1 to shared memory (read before
   // the first barrier below, used after it)
-  if constexpr (S::TWS > 0)
+  if (S::TWS > 0 && copy_tw)
   {
     const float4 *src = reinterpret_cast<const float4 *>(tw2);
     float4 *dst = reinterpret_cast<float4 *>(smem + S::SLOTS);
@@ -397,7 +402,6 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
   // prefetch into L2 the input of the tile that runs about one wave later
   if (a.ahead > 0)
   {
-    const long long tile = CL ? (long long)(blockIdx.x / S::CS) : (long long)blockIdx.x;
     const long long row0 = (tile + a.ahead) * S::ROWS;
     constexpr int LPR = S::N >= 16 ? S::N / 16 : 1;          // 128-byte lines per row
     constexpr int LINES = S::ROWS * LPR / S::CS;             // lines of this CTA's part
@@ -684,6 +688,17 @@ __global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
     }
     if constexpr (CL) cg::this_cluster().sync();
   }
+}
+
+// Standalone launch: one tile per CTA, or per cluster of CS CTAs.
+template <int LOGN, int MODE, int THREADS>
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
+{
+  using S = Sched<LOGN, THREADS>;
+  if constexpr (S::CS > 1)
+    row_tile<LOGN, MODE, THREADS>(a, blockIdx.x / S::CS, (int)cg::this_cluster().block_rank(), 0, true);
+  else
+    row_tile<LOGN, MODE, THREADS>(a, blockIdx.x, 0, 0, true);
 }
 
 }  // namespace fcb
