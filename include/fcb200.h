@@ -181,8 +181,10 @@ FCB_API int fcb_batch_create(int threads, fcb_batch *batch);
  * kinds); returns its id. */
 FCB_API int fcb_batch_add_replica(fcb_batch batch, const fcb_cf32 *replica, long long n,
                                   int replica_kind, int where, int *id);
-/* Define the job list (copied).  order 0: longest rows first (default load
- * balance), 1: as given.  Builds the job table and captures the graph. */
+/* Define the job list (copied).  order bit 0: 0 = longest rows first (default
+ * load balance), 1 = as given.  order bit 1 (value 2): launch directly instead
+ * of capturing a CUDA graph -- for job sets that change with every run, as in
+ * a serving loop; the job table is then copied on the batch's stream. */
 FCB_API int fcb_batch_set_jobs(fcb_batch batch, const fcb_job *jobs, int njobs, int order);
 /* Run all jobs once: one graph launch on the batch's stream (asynchronous). */
 FCB_API int fcb_batch_run(fcb_batch batch);

@@ -53,9 +53,11 @@ class Batch:
                                               _lib.FCB_HOST, ctypes.byref(rid)))
         return rid.value
 
-    def set_jobs(self, jobs, order: str = "longest_first") -> None:
+    def set_jobs(self, jobs, order: str = "longest_first", direct: bool = False) -> None:
         """jobs: iterable of (input, output, replica_id) with CUDA complex64
-        tensors of shape (pulses, n); output may be the input (in place)."""
+        tensors of shape (pulses, n); output may be the input (in place).
+        direct=True launches without capturing a CUDA graph (for job sets that
+        change with every run)."""
         arr = (FcbJob * max(1, len(jobs)))()
         keep = []
         for i, (x, y, rid) in enumerate(jobs):
@@ -70,8 +72,8 @@ class Batch:
             arr[i].n = x.shape[1]
             arr[i].replica = int(rid)
             keep.append((x, y))
-        check(lib().fcb_batch_set_jobs(self._h, ctypes.cast(arr, ctypes.c_void_p), len(jobs),
-                                       0 if order == "longest_first" else 1))
+        flags = (0 if order == "longest_first" else 1) | (2 if direct else 0)
+        check(lib().fcb_batch_set_jobs(self._h, ctypes.cast(arr, ctypes.c_void_p), len(jobs), flags))
         self._jobs = keep
 
     def set_stream(self, stream) -> None:

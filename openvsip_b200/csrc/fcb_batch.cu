@@ -154,6 +154,9 @@ struct fcb_batch_s
   struct Replica { float4 *table; int logn; };
   std::vector<Replica> replicas;
   BatchJob *d_jobs = nullptr;
+  size_t jobs_cap = 0;            // capacity of d_jobs (grown, never shrunk)
+  BatchJob *h_jobs = nullptr;     // pinned staging for the job table
+  bool direct = false;            // launch without a graph (job sets that change every run)
   int njobs = 0;
   long long total_units = 0;
   long long total_samples = 0;
@@ -190,6 +193,7 @@ void batch_free(fcb_batch b)
   for (auto &r : b->replicas) cudaFree(r.table);
   for (auto *t : b->tw) cudaFree(t);
   cudaFree(b->d_jobs);
+  cudaFreeHost(b->h_jobs);
   cudaFree(b->d_ticket);
   if (b->own_stream) cudaStreamDestroy(b->own_stream);
   delete b;
@@ -347,6 +351,8 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     if (j.pulses < 0 || (j.pulses > 0 && (!j.in || !j.out))) return set_error(FCB_ERR_INVALID, "job %d: bad buffers", i);
     if (j.in_rs < j.n || j.out_rs < j.n) return set_error(FCB_ERR_INVALID, "job %d: row stride < row length", i);
   }
+  const bool direct = (order & 2) != 0;
+  order &= 1;
   if (order == 0)  // longest rows first, then most rows: large units start early
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) {
       return jobs[a].n != jobs[c].n ? jobs[a].n > jobs[c].n : jobs[a].pulses > jobs[c].pulses;
@@ -385,17 +391,34 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     hj.push_back(bj);
   }
   cudaSetDevice(b->device);
+  // the previous run of this batch may still read the job table
   cudaStreamSynchronize(b->stream);
   drop_graph(b);
-  cudaFree(b->d_jobs);
-  b->d_jobs = nullptr;
   b->njobs = (int)hj.size();
   b->total_units = units;
   b->total_samples = samples;
+  b->direct = direct;
   if (hj.empty()) return FCB_OK;
-  cudaError_t e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * hj.size());
-  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "job table");
-  e = cudaMemcpy(b->d_jobs, hj.data(), sizeof(BatchJob) * hj.size(), cudaMemcpyHostToDevice);
+  if (hj.size() > b->jobs_cap)
+  {
+    cudaFree(b->d_jobs);
+    cudaFreeHost(b->h_jobs);
+    b->d_jobs = nullptr;
+    b->h_jobs = nullptr;
+    b->jobs_cap = 0;
+    const size_t cap = std::max<size_t>(hj.size(), 64);
+    cudaError_t e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * cap);
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "job table");
+    e = cudaMallocHost(&b->h_jobs, sizeof(BatchJob) * cap);
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "job table staging");
+    b->jobs_cap = cap;
+  }
+  std::copy(hj.begin(), hj.end(), b->h_jobs);
+  cudaError_t e = cudaMemcpyAsync(b->d_jobs, b->h_jobs, sizeof(BatchJob) * hj.size(), cudaMemcpyHostToDevice,
+                                  b->stream);
+  if (e != cudaSuccess) return cuda_error(e, "job table copy");
+  if (direct) return FCB_OK;
+  e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return cuda_error(e, "job table copy");
   return build_graph(b);
 }
@@ -404,8 +427,14 @@ int fcb_batch_run(fcb_batch b)
 {
   if (!b) return set_error(FCB_ERR_INVALID, "batch is NULL");
   if (b->njobs == 0) return FCB_OK;
-  if (!b->exec) return set_error(FCB_ERR_INVALID, "no jobs set");
   cudaSetDevice(b->device);
+  if (b->direct)
+  {
+    cudaError_t e = cudaMemsetAsync(b->d_ticket, 0, sizeof(unsigned long long), b->stream);
+    if (e != cudaSuccess) return cuda_error(e, "ticket reset");
+    return launch_batch(b, b->stream);
+  }
+  if (!b->exec) return set_error(FCB_ERR_INVALID, "no jobs set");
   cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
   if (e != cudaSuccess) return cuda_error(e, "graph launch");
   return FCB_OK;
