@@ -56,12 +56,21 @@ class Server:
     matched-filter spectra (kind "matched"), or spectra with kind="spectrum"."""
 
     def __init__(self, replicas, memory_budget: float = 40e9, slots: int = 2, max_jobs: int = 256,
-                 threads: int = 0, kind: str = "matched"):
+                 threads: int = 0, kind: str = "matched", reserve_bytes: float | None = None):
         import torch
         self.torch = torch
         self.budget = float(memory_budget)
         self.max_jobs = int(max_jobs)
         self.streams = [torch.cuda.Stream() for _ in range(slots)]
+        # Result buffers are allocated on the slot streams.  Reserve one large
+        # segment in each stream's pool of the caching allocator up front, so
+        # that serving splits cached memory instead of growing the pool with
+        # cudaMalloc (tens to hundreds of ms) while requests wait.
+        reserve = min(self.budget, 8e9) / slots if reserve_bytes is None else float(reserve_bytes)
+        for st in self.streams:
+            with torch.cuda.stream(st):
+                torch.empty(int(reserve) // 8, dtype=torch.complex64, device="cuda")
+        torch.cuda.synchronize()
         self.batches = []
         for st in self.streams:
             b = Batch(threads)
@@ -77,6 +86,9 @@ class Server:
         self._stop = False
         self.completed = 0
         self.launches = 0
+        self.issue_times = []  # host seconds spent issuing each launch
+        self.issue_parts = []  # (allocation, job table, launch) seconds and jobs, per launch
+        self._events = [torch.cuda.Event() for _ in range(slots)]
         self._thread = threading.Thread(target=self._loop, name="fcb-serve", daemon=True)
         self._thread.start()
 
@@ -143,19 +155,25 @@ class Server:
                     reqs = self._admit()
                 if not reqs:
                     break
+                t_issue = time.perf_counter()
                 try:
                     with torch.cuda.stream(self.streams[s]):
                         for r in reqs:
                             self.streams[s].wait_event(r.ready)
                             r.out = torch.empty_like(r.x)
                             r.t_start = time.perf_counter()
+                    t_alloc = time.perf_counter()
                     b = self.batches[s]
                     b.set_jobs([(r.x, r.out, r.replica) for r in reqs], direct=True)
+                    t_set = time.perf_counter()
                     b.run()
-                    ev = torch.cuda.Event()
+                    ev = self._events[s]
                     ev.record(self.streams[s])
                     self._inflight[s] = (reqs, ev)
                     self.launches += 1
+                    t_end = time.perf_counter()
+                    self.issue_times.append(t_end - t_issue)
+                    self.issue_parts.append((t_alloc - t_issue, t_set - t_alloc, t_end - t_set, len(reqs)))
                 except Exception as e:  # report to the clients, keep serving
                     with self._cv:
                         for r in reqs:
