@@ -238,6 +238,23 @@ def run_sweep(args):
                                   "samples_per_s": rows * n / (ms / 1e3), "gbs": gbs, "frac": gbs / peak,
                                   "threads": plan.info()["threads"], "cluster": plan.info()["cluster_ctas"]}),
                       flush=True)
+    # 4096 x 4096 2-D FFT, forward and inverse (two HBM passes each: 32 B/sample)
+    x = torch.randn(4096, 4096, dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(x)
+    for name, plan in (("fft2d_fwd", ov.Fft2d(4096, 4096, ov.fft_fwd)),
+                       ("fft2d_inv", ov.Fft2d(4096, 4096, ov.fft_inv, 1.0 / 4096 ** 2))):
+        for _ in range(3):
+            plan(x, y)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            plan(x, y)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1]) / args.steps
+        gbs = 32.0 * 4096 * 4096 / (ms / 1e3) / 1e9
+        print(json.dumps({"sweep": name, "n": 4096, "rows": 4096, "shape": "4096 x 4096", "ms": ms,
+                          "samples_per_s": 4096 * 4096 / (ms / 1e3), "gbs": gbs, "frac": gbs / peak}), flush=True)
 
 
 def _cgauss_dev(rows, n, gen):

@@ -97,6 +97,15 @@ FCB_API int fcb_supported_length(long long n);
 FCB_API int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale,
                   fcb_plan *plan);
 
+/* 2-D FFT plan over a rows x cols matrix (both powers of two in [64, 16384]),
+ * output times scale; fcb_exec then takes rows == the plan's rows.  Replaces
+ * fft_backend<2, complex<float>, complex<float>, S> (src/ovxx/signal/fft/
+ * backend.hpp:294-375; FFTW 2-D plan src/ovxx/fftw/fftw.cpp:436-511), used by
+ * vsip::Fft<const_Matrix, ...>.  Two passes, each a row transform that stores
+ * its result transposed; the plan keeps one rows x cols scratch matrix. */
+FCB_API int fcb_plan_fft2d(long long rows, long long cols, int exponent, float scale,
+                           fcb_plan *plan);
+
 /* Fused fast-convolution plan: y = IFFT(R .* FFT(x)) / n per row.
  * replica: replica_rows rows (1 = one vector shared by all rows, or one per
  * data row) of n samples at row stride replica_rs, kind fcb_replica_kind,

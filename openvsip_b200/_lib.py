@@ -63,6 +63,7 @@ SIGNATURES = {
     "fcb_supported_length": (c_int, [c_ll]),
     "fcb_plan_fftm": (c_int, [c_ll, c_ll, c_int, c_float, ctypes.POINTER(c_vp)]),
     "fcb_plan_fastconv": (c_int, [c_ll, c_ll, c_vp, c_ll, c_ll, c_int, c_int, ctypes.POINTER(c_vp)]),
+    "fcb_plan_fft2d": (c_int, [c_ll, c_ll, c_int, c_float, ctypes.POINTER(c_vp)]),
     "fcb_exec": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_int]),
     "fcb_set_stream": (c_int, [c_vp, c_vp]),
     "fcb_sync": (c_int, [c_vp]),

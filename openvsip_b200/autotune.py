@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import lib
 
 KINDS = {"forward": 0, "inverse": 1, "fastconv": 2}
-VARIANT_MIN_N = 8192  # 512-thread variants exist from 8192 samples up
+VARIANT_MIN_N = 4096  # 512-thread variants exist from 4096 samples up
 
 
 def cache_path() -> str:

@@ -180,7 +180,7 @@ static KernelInfo make_info()
   return k;
 }
 
-constexpr int kMin512 = 13;  // 512-thread variants exist for rows of 8192 samples and more
+constexpr int kMin512 = 12;  // 512-thread variants exist for rows of 4096 samples and more
 
 template <int LOGN>
 static void fill_table(KernelInfo (*tab)[3][2])
@@ -224,6 +224,14 @@ const KernelInfo *kernel_info(int logn, int mode)
   return &g_table[logn][mode][g_variant[logn][mode]];
 }
 
+const KernelInfo *kernel_variant(int logn, int mode, int threads)
+{
+  init_table();
+  if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return nullptr;
+  const int v = (threads == 512 && logn >= kMin512) ? 1 : 0;
+  return &g_table[logn][mode][v];
+}
+
 int set_variant(int logn, int mode, int threads)
 {
   init_table();
@@ -231,7 +239,7 @@ int set_variant(int logn, int mode, int threads)
     return set_error(FCB_ERR_INVALID, "bad length or mode for tuning");
   int v = threads == 512 ? 1 : threads == 256 ? 0 : -1;
   if (v < 0) return set_error(FCB_ERR_INVALID, "threads must be 256 or 512");
-  if (v == 1 && logn < kMin512) return set_error(FCB_ERR_UNSUPPORTED, "no 512-thread variant below 8192 samples");
+  if (v == 1 && logn < kMin512) return set_error(FCB_ERR_UNSUPPORTED, "no 512-thread variant below 4096 samples");
   std::lock_guard<std::mutex> lk(g_variant_mu);
   g_variant[logn][mode] = v;
   return FCB_OK;

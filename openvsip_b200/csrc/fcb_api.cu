@@ -28,6 +28,14 @@ struct fcb_plan_s
   float2 *stage[2] = {nullptr, nullptr};
   long long stage_rows = 0;
   cudaEvent_t done[2] = {nullptr, nullptr};
+  // 2-D FFT (rows x cols): pass 1 transforms rows into a transposed scratch
+  // matrix, pass 2 transforms its rows (the columns) back transposed.
+  bool is2d = false;
+  long long rows2d = 0, cols2d = 0;
+  const KernelInfo *kc = nullptr;  // pass 2 kernel (length rows2d)
+  float4 *twc = nullptr;
+  float2 *scratch = nullptr;
+  float2 *stage2d_in = nullptr, *stage2d_out = nullptr;
 };
 
 namespace {
@@ -77,6 +85,10 @@ void plan_free(fcb_plan p)
   if (p->own_stream) cudaStreamSynchronize(p->own_stream);
   if (p->aux) cudaStreamSynchronize(p->aux);
   cudaFree(p->tw);
+  cudaFree(p->twc);
+  cudaFree(p->scratch);
+  cudaFree(p->stage2d_in);
+  cudaFree(p->stage2d_out);
   cudaFree(p->rep);
   cudaFree(p->stage[0]);
   cudaFree(p->stage[1]);
@@ -109,6 +121,31 @@ int plan_common(fcb_plan p, long long n, long long rows_max, int mode)
   return FCB_OK;
 }
 
+// 2-D FFT on device pointers: two transposing row passes.
+int exec_2d(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs, cudaStream_t st)
+{
+  RowArgs a = {};
+  a.in = in;
+  a.in_rs = in_rs;
+  a.out = p->scratch;
+  a.out_rs = p->rows2d;
+  a.rows = p->rows2d;
+  a.tw = a.twi = p->tw;
+  a.scale = 1.f;
+  a.transpose_out = 1;
+  a.ahead = -1;
+  int rc = launch_rows(p->k, p->rows2d, a, st);
+  if (rc) return rc;
+  a.in = p->scratch;
+  a.in_rs = p->rows2d;
+  a.out = out;
+  a.out_rs = out_rs;
+  a.rows = p->cols2d;
+  a.tw = a.twi = p->twc;
+  a.scale = p->scale;
+  return launch_rows(p->kc, p->cols2d, a, st);
+}
+
 // Device-pointer execution on stream st.
 int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
                 long long rows, long long row0, cudaStream_t st)
@@ -118,7 +155,7 @@ int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long
   if (p->logn == 0)
     return launch_scale_rows(in, in_rs, out, out_rs, rows, p->mode == kFastconv ? rep : nullptr, rep_rs,
                              p->scale, st);
-  RowArgs a;
+  RowArgs a = {};
   a.in = in;
   a.in_rs = in_rs;
   a.out = out;
@@ -333,6 +370,29 @@ int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, lon
   DeviceGuard g(p->device);
   const float2 *i2 = reinterpret_cast<const float2 *>(in);
   float2 *o2 = reinterpret_cast<float2 *>(out);
+  if (p->is2d)
+  {
+    if (rows != p->rows2d) return set_error(FCB_ERR_INVALID, "a 2-D FFT transforms the whole %lld-row matrix", p->rows2d);
+    if ((const void *)in == (const void *)out && in_rs != out_rs)
+      return set_error(FCB_ERR_INVALID, "in-place call with different row strides");
+    if (where == FCB_DEVICE) return exec_2d(p, i2, in_rs, o2, out_rs, p->stream);
+    const size_t bytes = sizeof(float2) * (size_t)(p->rows2d * p->cols2d);
+    cudaError_t e = cudaSuccess;
+    if (!p->stage2d_in && (e = cudaMalloc(&p->stage2d_in, bytes)) != cudaSuccess)
+      return set_error(FCB_ERR_NOMEM, "staging buffer: %s", cudaGetErrorString(e));
+    const size_t rb = sizeof(float2) * (size_t)p->cols2d;
+    e = cudaMemcpy2DAsync(p->stage2d_in, rb, i2, sizeof(float2) * (size_t)in_rs, rb, (size_t)p->rows2d,
+                          cudaMemcpyHostToDevice, p->stream);
+    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    int rc = exec_2d(p, p->stage2d_in, p->cols2d, p->stage2d_in, p->cols2d, p->stream);
+    if (rc) return rc;
+    e = cudaMemcpy2DAsync(o2, sizeof(float2) * (size_t)out_rs, p->stage2d_in, rb, rb, (size_t)p->rows2d,
+                          cudaMemcpyDeviceToHost, p->stream);
+    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) return cuda_error(e, "fcb_exec (2-D, host)");
+    return FCB_OK;
+  }
   if (where == FCB_DEVICE) return exec_device(p, i2, in_rs, o2, out_rs, rows, 0, p->stream);
   return exec_host(p, i2, in_rs, o2, out_rs, rows);
 }
@@ -368,6 +428,48 @@ int fcb_plan_info(fcb_plan p, long long *n, int *cluster_ctas, int *rows_per_cta
   if (cluster_ctas) *cluster_ctas = p->k ? p->k->cluster : 1;
   if (rows_per_cta) *rows_per_cta = p->k ? p->k->rows_per_cta : 1;
   if (smem_bytes) *smem_bytes = p->k ? p->k->smem : 0;
+  return FCB_OK;
+}
+
+int fcb_plan_fft2d(long long rows, long long cols, int exponent, float scale, fcb_plan *plan)
+{
+  if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
+  *plan = nullptr;
+  const int lr = log2_exact(rows), lc = log2_exact(cols);
+  if (lr < 6 || lr > 14 || lc < 6 || lc > 14)
+    return set_error(FCB_ERR_UNSUPPORTED, "2-D FFT dimensions must be powers of two in [64, 16384], got %lld x %lld",
+                     rows, cols);
+  if (exponent != FCB_FORWARD && exponent != FCB_INVERSE) return set_error(FCB_ERR_INVALID, "exponent must be -1 or +1");
+  fcb_plan p = new (std::nothrow) fcb_plan_s;
+  if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
+  const int mode = exponent == FCB_FORWARD ? kFwd : kInv;
+  p->scale = scale;
+  p->is2d = true;
+  p->rows2d = rows;
+  p->cols2d = cols;
+  int rc = plan_common(p, cols, rows, mode);
+  if (!rc)
+  {
+    // 512-thread CTAs hold 4 rows of 4096 (or more of shorter rows), so each
+    // transposed store writes whole 32-byte sectors
+    p->k = kernel_variant(lc, mode, 512);
+    p->kc = kernel_variant(lr, mode, 512);
+    rc = prepare_kernel(p->k);
+    if (!rc) rc = prepare_kernel(p->kc);
+    if (!rc) rc = build_twiddles(lr, &p->twc, p->stream);  // pass-2 table (length rows)
+  }
+  if (!rc)
+  {
+    cudaError_t e = cudaMalloc(&p->scratch, sizeof(float2) * (size_t)(rows * cols));
+    if (e != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "2-D scratch: %s", cudaGetErrorString(e));
+  }
+  if (!rc)
+  {
+    cudaError_t e = cudaStreamSynchronize(p->stream);
+    if (e != cudaSuccess) rc = cuda_error(e, "plan tables");
+  }
+  if (rc) { plan_free(p); return rc; }
+  *plan = p;
   return FCB_OK;
 }
 

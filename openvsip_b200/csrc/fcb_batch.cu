@@ -363,7 +363,7 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     const fcb_job &j = jobs[i];
     if (j.pulses == 0) continue;
     const int l = b->replicas[j.replica].logn;
-    BatchJob bj;
+    BatchJob bj = {};
     bj.logn = l;
     // geometry of this length on the variant's CTAs (as in Sched<>)
     const int T = b->v.threads;

@@ -310,6 +310,7 @@ struct RowArgs
   const float4 *rep;    // fused: replica pair table (slot order, scaled 1/N)
   long long rep_rs;     // fused: replica row stride in slots (0 = one vector)
   float scale;          // standalone: output scale
+  int transpose_out;    // standalone FFT: store the result transposed (2-D FFT passes)
   long long ahead;      // L2 prefetch distance in tiles (CTAs, or clusters) -- about
                         // one resident wave, so that tile's rows stream from HBM
                         // into L2 while this tile computes; 0 = off
@@ -560,6 +561,32 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     const int tl = t % S::TPRL;
     float2 *dstp = a.out + row * a.out_rs;
     const float2 sc = f2dup(a.scale);
+    if constexpr (!CL && S::NS > 1)
+    {
+      if (a.transpose_out)
+      {
+        // Transposed store (one pass of a 2-D FFT): element (row, k) goes to
+        // out[k * out_rs + row].  Consecutive threads take consecutive rows of
+        // this CTA for the same frequency pair, so a warp writes ROWS
+        // consecutive elements of each output row it touches.
+        const long long row0 = tile * S::ROWS;
+#pragma unroll
+        for (int i = 0; i < S::CPT; ++i)
+        {
+          const int idx = t + THREADS * i;
+          const int rr = idx % S::ROWS, m = idx / S::ROWS;
+          cpair p = cp_from4(ld_slot<false>(slot_addr(rr * S::HALF + m)));
+          p.re = f2mul(p.re, sc);
+          p.im = f2mul(p.im, sc);
+          if (row0 + rr < a.rows)
+          {
+            a.out[(2LL * m) * a.out_rs + row0 + rr] = make_float2(p.re.x, p.im.x);
+            a.out[(2LL * m + 1) * a.out_rs + row0 + rr] = make_float2(p.re.y, p.im.y);
+          }
+        }
+        return;
+      }
+    }
 #pragma unroll
     for (int i = 0; i < S::CPT; ++i)
     {

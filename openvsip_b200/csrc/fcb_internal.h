@@ -28,6 +28,7 @@ struct KernelInfo
 
 const KernelInfo *kernel_info(int logn, int mode);
 int set_variant(int logn, int mode, int threads);
+const KernelInfo *kernel_variant(int logn, int mode, int threads);
 int get_variant(int logn, int mode);
 int prepare_kernel(const KernelInfo *k);
 int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaStream_t st);

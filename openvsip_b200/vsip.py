@@ -147,6 +147,25 @@ class Fftm(_Plan):
         return self._exec(inout, inout)
 
 
+class Fft2d(_Plan):
+    """2-D FFT of a rows x cols matrix on the GPU (vsip::Fft<const_Matrix, C, C,
+    D>, src/vsip/impl/signal/fft.hpp:75-132): rows, then columns, output times
+    scale.  Dimensions: powers of two in [64, 16384]."""
+
+    def __init__(self, rows: int, cols: int, direction: int = fft_fwd, scale: float = 1.0):
+        self.rows, self.cols = int(rows), int(cols)
+        self.exponent = _exponent(direction)
+        self.scale = float(scale)
+        h = ctypes.c_void_p()
+        check(lib().fcb_plan_fft2d(self.rows, self.cols, self.exponent, self.scale, ctypes.byref(h)))
+        self._handle = h
+
+    def __call__(self, inp, out=None):
+        if out is None:
+            out = _empty_like(inp)
+        return self._exec(inp, out)
+
+
 class Fastconv(_Plan):
     """Fused fast convolution: ``inv_fftm(vmmul<0>(weights, for_fftm(in)))``.
 
@@ -218,5 +237,5 @@ def supported_length(n: int) -> bool:
     return bool(lib().fcb_supported_length(int(n)))
 
 
-__all__ = ["Fftm", "Fastconv", "vmmul", "replica_spectrum", "supported_length", "fft_fwd", "fft_inv",
+__all__ = ["Fftm", "Fft2d", "Fastconv", "vmmul", "replica_spectrum", "supported_length", "fft_fwd", "fft_inv",
            "FcbError"]
