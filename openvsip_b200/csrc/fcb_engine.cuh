@@ -392,12 +392,16 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 
   // copy the twiddle tables of stages 2..NS-1 to shared memory (read before
   // the first barrier below, used after it)
+  // with asynchronous copies (no register round trip, nothing waits on them
+  // before the barrier that ends stage 1)
   if (S::TWS > 0 && copy_tw)
   {
     const float4 *src = reinterpret_cast<const float4 *>(tw2);
-    float4 *dst = reinterpret_cast<float4 *>(smem + S::SLOTS);
 #pragma unroll 4
-    for (int i = t; i < S::TWS / 2; i += THREADS) dst[i] = __ldg(src + i);
+    for (int i = t; i < S::TWS / 2; i += THREADS)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                   :: "r"(tw_base + 16u * i), "l"(src + i) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
   }
 
   // prefetch into L2 the input of the tile that runs about one wave later
@@ -469,6 +473,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   }
   if constexpr (S::NS > 1)
   {
+    if (S::TWS > 0 && copy_tw) asm volatile("cp.async.wait_all;" ::: "memory");
     if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
   }
 
@@ -657,19 +662,18 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     if constexpr (S::NS >= 3) stage_inv(ic<3>{});
     if constexpr (S::NS >= 2) stage_inv(ic<2>{});
 
-    if constexpr (S::NS > 1)
-    {
-      if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
-    }
-
-    // ---------------- inverse stage 1 and store ----------------
-    float2 *dstp = a.out + row * a.out_rs;
+    // inverse stage-1 twiddles: issued before the barrier so that its wait
+    // covers their latency
     float4 tw1[S::H1];
     if constexpr (S::NS > 1)
     {
 #pragma unroll
       for (int qp = 0; qp < S::H1; ++qp) tw1[qp] = ldv4(a.twi + qp * S::D + tr);
+      if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
     }
+
+    // ---------------- inverse stage 1 and store ----------------
+    float2 *dstp = a.out + row * a.out_rs;
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
     {
