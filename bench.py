@@ -220,9 +220,10 @@ def run_sweep(args):
             x = (torch.randn(rows, n, dtype=torch.complex64, device="cuda"))
             y = torch.empty_like(x)
             rep = np.ones(n, dtype=np.complex64)
+            if args.threads:
+                for kind_id in (0, 2):
+                    ov.lib().fcb_tune_set(n, kind_id, args.threads)
             for kind, plan in (("fastconv", ov.Fastconv(rep, rows)), ("fftm_fwd", ov.Fftm(rows, n, ov.fft_fwd))):
-                if args.threads:
-                    pass
                 for _ in range(3):
                     plan(x, y)
                 ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]

@@ -181,9 +181,10 @@ static KernelInfo make_info()
 }
 
 constexpr int kMin512 = 12;  // 512-thread variants exist for rows of 4096 samples and more
+constexpr int kMin128 = 8, kMax128 = 14;  // 128-thread variants: rows of 256 .. 16384 samples
 
 template <int LOGN>
-static void fill_table(KernelInfo (*tab)[3][2])
+static void fill_table(KernelInfo (*tab)[3][3])
 {
   if constexpr (LOGN >= 1)
   {
@@ -196,11 +197,17 @@ static void fill_table(KernelInfo (*tab)[3][2])
       tab[LOGN][kInv][1] = make_info<LOGN, kInv, 512>();
       tab[LOGN][kFastconv][1] = make_info<LOGN, kFastconv, 512>();
     }
+    if constexpr (LOGN >= kMin128 && LOGN <= kMax128)
+    {
+      tab[LOGN][kFwd][2] = make_info<LOGN, kFwd, 128>();
+      tab[LOGN][kInv][2] = make_info<LOGN, kInv, 128>();
+      tab[LOGN][kFastconv][2] = make_info<LOGN, kFastconv, 128>();
+    }
     fill_table<LOGN - 1>(tab);
   }
 }
 
-static KernelInfo g_table[kMaxLogN + 1][3][2];
+static KernelInfo g_table[kMaxLogN + 1][3][3];
 static std::once_flag g_table_once;
 // Variant chosen per (logn, mode); set by the autotuner through fcb_tune_set.
 static int g_variant[kMaxLogN + 1][3];
@@ -212,7 +219,9 @@ static void init_table()
     fill_table<kMaxLogN>(g_table);
     for (int l = 0; l <= kMaxLogN; ++l)
       for (int m = 0; m < 3; ++m)
-        g_variant[l][m] = (l == 14) ? 1 : 0;  // default: one 512-thread CTA per 16384-sample row
+        // defaults (measured): 4 CTAs of 128 threads per SM for rows of 256 ..
+        // 4096 samples, one 512-thread CTA per 16384-sample row, else 256
+        g_variant[l][m] = (l == 14) ? 1 : (l >= kMin128 && l <= kMax128) ? 2 : 0;
   });
 }
 
@@ -228,7 +237,8 @@ const KernelInfo *kernel_variant(int logn, int mode, int threads)
 {
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return nullptr;
-  const int v = (threads == 512 && logn >= kMin512) ? 1 : 0;
+  const int v = (threads == 512 && logn >= kMin512) ? 1
+              : (threads == 128 && logn >= kMin128 && logn <= kMax128) ? 2 : 0;
   return &g_table[logn][mode][v];
 }
 
@@ -237,9 +247,11 @@ int set_variant(int logn, int mode, int threads)
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2)
     return set_error(FCB_ERR_INVALID, "bad length or mode for tuning");
-  int v = threads == 512 ? 1 : threads == 256 ? 0 : -1;
-  if (v < 0) return set_error(FCB_ERR_INVALID, "threads must be 256 or 512");
+  int v = threads == 512 ? 1 : threads == 256 ? 0 : threads == 128 ? 2 : -1;
+  if (v < 0) return set_error(FCB_ERR_INVALID, "threads must be 128, 256 or 512");
   if (v == 1 && logn < kMin512) return set_error(FCB_ERR_UNSUPPORTED, "no 512-thread variant below 4096 samples");
+  if (v == 2 && (logn < kMin128 || logn > kMax128))
+    return set_error(FCB_ERR_UNSUPPORTED, "128-thread variants exist for 256 .. 16384 samples");
   std::lock_guard<std::mutex> lk(g_variant_mu);
   g_variant[logn][mode] = v;
   return FCB_OK;
@@ -250,7 +262,7 @@ int get_variant(int logn, int mode)
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return 0;
   std::lock_guard<std::mutex> lk(g_variant_mu);
-  return g_variant[logn][mode] ? 512 : 256;
+  return g_variant[logn][mode] == 1 ? 512 : g_variant[logn][mode] == 2 ? 128 : 256;
 }
 
 int prepare_kernel(const KernelInfo *k)

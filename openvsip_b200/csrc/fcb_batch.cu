@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(T, 512 / T)
     long long u;
     if constexpr (HC)
     {
-      cg::this_cluster().sync();
+      cluster_sync();
       u = ld_cluster_s64(cluster_addr(smem_addr(&s_unit[it & 1]), 0));
     }
     else
@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(T, 512 / T)
     }
     if (u >= total_units)
     {
-      if constexpr (HC) cg::this_cluster().sync();  // rank 0 stays until every CTA has read
+      if constexpr (HC) cluster_sync();  // rank 0 stays until every CTA has read
       break;
     }
     int lo = 0, hi = njobs - 1;

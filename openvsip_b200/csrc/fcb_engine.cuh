@@ -88,7 +88,7 @@ struct Sched
   }
   __host__ __device__ static constexpr int tw_bytes() { return HALF * 16 + tw2_off(NS + 1) * 8; }
   static constexpr int TWS = NS >= 3 ? tw2_off(NS) : 0;   // float2 entries kept in shared memory
-  static constexpr int SMEM = SLOTS * 16 + TWS * 8;
+  static constexpr int SMEM = (SLOTS + SLOTS / 16) * 16 + TWS * 8;  // padded slots, then twiddles
 };
 
 
@@ -220,8 +220,13 @@ __host__ __device__ __forceinline__ int digitrev16(int p, int ndig)
   return r;
 }
 
-// Shared-memory slot swizzle (16-byte slots, 8 slots per 128-byte bank row).
-__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 7); }
+// Physical position of slot i in shared memory: one padding slot after every
+// 16 slots.  Every exchange pattern of the kernel (consecutive slots across
+// threads, slots 16 apart across threads for the last stage) then falls on
+// distinct 16-byte banks, and for the stride patterns of a stage the physical
+// address stays linear in the element index, so the compiler folds the
+// per-element offsets into the load/store instructions.
+__device__ __forceinline__ int swz(int i) { return i + (i >> 4); }
 
 // Loads that stay where they are written: volatile asm is not moved across
 // other volatile asm or memory operations, so twiddle and replica loads are
@@ -337,6 +342,13 @@ struct SlotMap
 template <int S_>
 using ic = std::integral_constant<int, S_>;
 
+// Cluster-wide barrier with release/acquire ordering of shared::cluster
+// accesses; every thread of every CTA of the cluster executes it.
+__device__ __forceinline__ void cluster_sync()
+{
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 // Barrier over the NT consecutive threads that share one exchange (NT a power
 // of two dividing THREADS): a warp barrier when they sit in one warp, a named
 // barrier per group otherwise, the CTA barrier when the group is the CTA.
@@ -387,7 +399,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     for (int r = 0; r < S::CS; ++r) peer[r] = cluster_addr(own, rank_base + r);
   }
   const uint32_t slot_base = smem_addr(smem);
-  const uint32_t tw_base = slot_base + 16u * S::SLOTS;  // later-stage twiddles in shared memory
+  const uint32_t tw_base = slot_base + 16u * (S::SLOTS + S::SLOTS / 16);  // later-stage twiddles
   auto slot_addr = [&](int local) { return slot_base + 16u * (uint32_t)swz(local); };
 
   // copy the twiddle tables of stages 2..NS-1 to shared memory (read before
@@ -474,7 +486,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   if constexpr (S::NS > 1)
   {
     if (S::TWS > 0 && copy_tw) asm volatile("cp.async.wait_all;" ::: "memory");
-    if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+    if constexpr (CL) cluster_sync(); else __syncthreads();
   }
 
   // ---------------- stages 2..NS, direction SIGN ----------------
@@ -554,14 +566,14 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         dst[i] = sigma / S::D + S::H1 * digitrev16(sigma % S::D, S::NS - 1);
       }
     }
-    if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+    if constexpr (CL) cluster_sync(); else __syncthreads();
 #pragma unroll
     for (int i = 0; i < S::CPT; ++i)
     {
       const int m = dst[i];
       st_slot<CL>(peer[SlotMap<S>::owner(m)] + 16u * swz(SlotMap<S>::local(m, rho)), cp_to4(c[i]));
     }
-    if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+    if constexpr (CL) cluster_sync(); else __syncthreads();
     // natural-order read of this CTA's part of the row, scale, store.
     const int tl = t % S::TPRL;
     float2 *dstp = a.out + row * a.out_rs;
@@ -669,11 +681,25 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     {
 #pragma unroll
       for (int qp = 0; qp < S::H1; ++qp) tw1[qp] = ldv4(a.twi + qp * S::D + tr);
-      if constexpr (CL) cg::this_cluster().sync(); else __syncthreads();
+      if constexpr (CL) cluster_sync(); else __syncthreads();
     }
 
     // ---------------- inverse stage 1 and store ----------------
     float2 *dstp = a.out + row * a.out_rs;
+    // all slot reads of this thread first (remote ones in a cluster have a long
+    // round trip; issuing them together overlaps their latencies)
+    float4 v[S::CPT];
+    if constexpr (S::NS > 1)
+    {
+#pragma unroll
+      for (int g = 0; g < S::G1; ++g)
+#pragma unroll
+        for (int qp = 0; qp < S::H1; ++qp)
+        {
+          const int sigma = qp * S::D + tr + S::TPR * g;
+          v[g * S::H1 + qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)));
+        }
+    }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
     {
@@ -681,16 +707,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       cpair z[S::H1];
       if constexpr (S::NS > 1)
       {
-        float4 v[S::H1];
 #pragma unroll
         for (int qp = 0; qp < S::H1; ++qp)
-        {
-          const int sigma = qp * S::D + n;
-          v[qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)));
-        }
-#pragma unroll
-        for (int qp = 0; qp < S::H1; ++qp)
-          z[qp] = cp_rot2<+1>(cp_mul4c(cp_from4(v[qp]), tw1[qp]), (g * 2 * qp) & 31, (g * (2 * qp + 1)) & 31);
+          z[qp] = cp_rot2<+1>(cp_mul4c(cp_from4(v[g * S::H1 + qp]), tw1[qp]), (g * 2 * qp) & 31,
+                              (g * (2 * qp + 1)) & 31);
       }
       else
       {
@@ -717,7 +737,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         }
       }
     }
-    if constexpr (CL) cg::this_cluster().sync();
+    if constexpr (CL) cluster_sync();
   }
 }
 
