@@ -89,11 +89,19 @@ FCB_API const char *fcb_last_error(void);
 FCB_API const char *fcb_version(void);
 /* Select the CUDA device for subsequent plans of the calling thread. */
 FCB_API int fcb_init(int device);
-/* 1 if n is a supported row length. */
+/* 1 if n is a supported row length for Fftm and fast-convolution plans: any
+ * length in [1, 32768], or a power of two up to 65536.  Powers of two run as
+ * one fused pass; other lengths by Bluestein's chirp-z algorithm over work
+ * rows of the next power of two >= 2n - 1 samples (a chirp pre-multiply, one
+ * fused pass per transform, a chirp post-multiply).  The reference's FFTW
+ * backend plans any length (src/ovxx/fftw/fftw.cpp:39-116). */
 FCB_API int fcb_supported_length(long long n);
 
 /* Row-wise multiple FFT plan: n samples per row, up to rows_max rows per call,
- * exponent FCB_FORWARD or FCB_INVERSE, output multiplied by scale. */
+ * exponent FCB_FORWARD or FCB_INVERSE, output multiplied by scale.  Replaces
+ * fftm_backend<complex<float>, complex<float>, 0, D> (src/ovxx/signal/fft/
+ * backend.hpp:696-784; FFTW plan src/ovxx/fftw/fftw.cpp:904-1001).  A
+ * non-power-of-two plan keeps a work buffer of at most 2^25 samples. */
 FCB_API int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale,
                   fcb_plan *plan);
 
@@ -147,7 +155,8 @@ FCB_API int fcb_vmmul_rows(const fcb_cf32 *v, const fcb_cf32 *m, long long m_rs,
                    long long cols, void *stream);
 
 /* Replica spectrum in FP64 on the GPU, rounded to complex<float>:
- * spectrum = FFT(replica) or conj(FFT(replica)) (matched), n a power of two.
+ * spectrum = FFT(replica) or conj(FFT(replica)) (matched), n a supported
+ * length (radix-2 FFT for powers of two, a direct DFT otherwise).
  * Device pointers; synchronous. */
 FCB_API int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int matched,
                          fcb_cf32 *spectrum_dev);

@@ -135,6 +135,46 @@ __global__ void fft_fp64_kernel(const float2 *in, double2 *buf0, double2 *buf1, 
     out[i] = make_float2((float)src[i].x, (float)(matched ? -src[i].y : src[i].y));
 }
 
+// FP64 DFT of one vector of non-power-of-two length n <= 32768 (so j * k
+// stays below 2^30), one CTA per output bin; w[m] = e^{-2 pi i m / n}.
+// Plan-time only (replica spectra of Bluestein plans).
+__global__ void dft_table_kernel(double2 *w, long long n)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double sn, cs;
+  sincospi(-2.0 * (double)i / (double)n, &sn, &cs);
+  w[i] = make_double2(cs, sn);
+}
+
+__global__ void dft_fp64_kernel(const float2 *in, const double2 *w, unsigned n, int matched, float2 *out)
+{
+  __shared__ double part[2][32];
+  const unsigned k = blockIdx.x;
+  double re = 0.0, im = 0.0;
+  for (unsigned j = threadIdx.x; j < n; j += blockDim.x)
+  {
+    const double2 t = w[(j * k) % n];
+    const float2 x = in[j];
+    re += (double)x.x * t.x - (double)x.y * t.y;
+    im += (double)x.x * t.y + (double)x.y * t.x;
+  }
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    re += __shfl_xor_sync(0xffffffffu, re, o);
+    im += __shfl_xor_sync(0xffffffffu, im, o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { part[0][warp] = re; part[1][warp] = im; }
+  __syncthreads();
+  if (threadIdx.x == 0)
+  {
+    re = im = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) { re += part[0][i]; im += part[1][i]; }
+    out[k] = make_float2((float)re, (float)(matched ? -im : im));
+  }
+}
+
 __global__ void vmmul_kernel(const float2 *v, const float2 *m, long long m_rs, float2 *out,
                              long long out_rs, long long rows, long long cols)
 {
@@ -221,7 +261,8 @@ static void init_table()
       for (int m = 0; m < 3; ++m)
         // defaults (measured): 4 CTAs of 128 threads per SM for rows of 256 ..
         // 4096 samples, one 512-thread CTA per 16384-sample row, else 256
-        g_variant[l][m] = (l == 14) ? 1 : (l >= kMin128 && l <= kMax128) ? 2 : 0;
+        // (128-thread clusters for 8192 and 16384 samples measured slower)
+        g_variant[l][m] = (l == 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
   });
 }
 
@@ -340,7 +381,18 @@ int replica_spectrum_dev(const float2 *rep_dev, long long n, int matched, float2
   double2 *buf = nullptr;
   cudaError_t e = cudaMallocAsync(&buf, sizeof(double2) * 2 * (size_t)n, st);
   if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "replica FFT buffer: %s", cudaGetErrorString(e));
-  fft_fp64_kernel<<<1, 1024, 0, st>>>(rep_dev, buf, buf + n, n, matched, spec_dev);
+  if ((n & (n - 1)) == 0)
+    fft_fp64_kernel<<<1, 1024, 0, st>>>(rep_dev, buf, buf + n, n, matched, spec_dev);
+  else if (n <= 32768)
+  {
+    dft_table_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(buf, n);
+    dft_fp64_kernel<<<(unsigned)n, 256, 0, st>>>(rep_dev, buf, (unsigned)n, matched, spec_dev);
+  }
+  else
+  {
+    cudaFreeAsync(buf, st);
+    return set_error(FCB_ERR_UNSUPPORTED, "replica length %lld: not a power of two and above 32768", n);
+  }
   e = cudaGetLastError();
   cudaFreeAsync(buf, st);
   if (e != cudaSuccess) return cuda_error(e, "replica FFT");

@@ -36,6 +36,15 @@ struct fcb_plan_s
   float4 *twc = nullptr;
   float2 *scratch = nullptr;
   float2 *stage2d_in = nullptr, *stage2d_out = nullptr;
+  // Rows of non-power-of-two length n (Bluestein): chirp pre-multiply into
+  // work rows of blue_m >= 2n - 1 samples, fused length-blue_m pass(es),
+  // chirp post-multiply.  Index 0 is the forward direction, 1 the inverse.
+  long long blue_m = 0;
+  long long blue_chunk = 0;                    // rows per work-buffer pass
+  float2 *chirp[2] = {nullptr, nullptr};       // c[k] = e^{-+ i pi k^2 / n}
+  fcb_plan inner[2] = {nullptr, nullptr};      // length-blue_m fastconv, replica FFT(conj(c))
+  float2 *blue_rep = nullptr;                  // fastconv: replica spectra / n, rows of n
+  float2 *blue_buf[2] = {nullptr, nullptr};    // work rows, one per staging stream
 };
 
 namespace {
@@ -47,6 +56,14 @@ int log2_exact(long long n)
   while ((1LL << l) < n) ++l;
   return l;
 }
+
+// Non-power-of-two lengths up to half the longest fused row run by Bluestein.
+constexpr long long kMaxBlueN = 1LL << (kMaxLogN - 1);
+constexpr long long kBlueChunkSamples = 1LL << 25;  // work buffer: 256 MiB at most
+
+bool blue_length(long long n) { return n > 0 && n <= kMaxBlueN && (n & (n - 1)) != 0; }
+
+#define FCB_LENGTH_RULE "any length in [1, 32768], or a power of two up to 65536"
 
 struct DeviceGuard
 {
@@ -92,6 +109,13 @@ void plan_free(fcb_plan p)
   cudaFree(p->rep);
   cudaFree(p->stage[0]);
   cudaFree(p->stage[1]);
+  for (int d = 0; d < 2; ++d)
+  {
+    plan_free(p->inner[d]);
+    cudaFree(p->chirp[d]);
+    cudaFree(p->blue_buf[d]);
+  }
+  cudaFree(p->blue_rep);
   for (auto &e : p->done) if (e) cudaEventDestroy(e);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
   if (p->aux) cudaStreamDestroy(p->aux);
@@ -121,6 +145,77 @@ int plan_common(fcb_plan p, long long n, long long rows_max, int mode)
   return FCB_OK;
 }
 
+// Bluestein plan for non-power-of-two n: a chirp and an inner length-m
+// fastconv plan per direction needed (fwd / inv), and one work buffer.
+int blue_setup(fcb_plan p, long long n, long long rows_max, int mode, bool need_fwd, bool need_inv)
+{
+  int rc = check_device();
+  if (rc) return rc;
+  cudaGetDevice(&p->device);
+  p->n = n;
+  p->logn = -1;
+  p->mode = mode;
+  p->rows_max = rows_max;
+  cudaError_t e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cuda_error(e, "cudaStreamCreate");
+  p->stream = p->own_stream;
+  long long m = 1;
+  while (m < 2 * n - 1) m <<= 1;
+  p->blue_m = m;
+  p->blue_chunk = std::max<long long>(1, std::min(rows_max, kBlueChunkSamples / m));
+  for (int d = 0; d < 2; ++d)
+  {
+    if (!(d == 0 ? need_fwd : need_inv)) continue;
+    float2 *spec = nullptr;
+    rc = bluestein_tables(n, m, d == 0 ? -1 : +1, &p->chirp[d], &spec, p->stream);
+    if (rc) return rc;
+    rc = fcb_plan_fastconv(m, p->blue_chunk, reinterpret_cast<const fcb_cf32 *>(spec), 1, m, FCB_REPLICA_SPECTRUM,
+                           FCB_DEVICE, &p->inner[d]);
+    cudaFree(spec);
+    if (rc) return rc;
+  }
+  e = cudaMalloc(&p->blue_buf[0], sizeof(float2) * (size_t)(p->blue_chunk * m));
+  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "Bluestein work rows: %s", cudaGetErrorString(e));
+  return FCB_OK;
+}
+
+int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
+                long long rows, long long row0, cudaStream_t st, int slot = 0);
+
+// Bluestein execution on stream st with work buffer `slot`, in chunks of
+// blue_chunk rows.  In place is fine: a chunk reads its input rows before it
+// writes the same rows.
+int exec_blue(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
+              long long row0, cudaStream_t st, int slot)
+{
+  float2 *buf = p->blue_buf[slot];
+  const long long n = p->n, m = p->blue_m;
+  int rc = FCB_OK;
+  for (long long r0 = 0; !rc && r0 < rows; r0 += p->blue_chunk)
+  {
+    const long long nr = std::min(p->blue_chunk, rows - r0);
+    const float2 *x = in + r0 * in_rs;
+    float2 *y = out + r0 * out_rs;
+    if (p->mode == kFastconv)
+    {
+      const bool per_row = p->rep_rows > 1;
+      rc = bluestein_pre(x, in_rs, p->chirp[0], buf, n, m, nr, st);
+      if (!rc) rc = exec_device(p->inner[0], buf, m, buf, m, nr, 0, st);
+      if (!rc) rc = bluestein_mid(buf, m, p->blue_rep + (per_row ? (row0 + r0) * n : 0), per_row ? n : 0, n, nr, st);
+      if (!rc) rc = exec_device(p->inner[1], buf, m, buf, m, nr, 0, st);
+      if (!rc) rc = bluestein_post(buf, m, p->chirp[1], y, out_rs, n, nr, 1.f, st);
+    }
+    else
+    {
+      const int d = p->mode == kFwd ? 0 : 1;
+      rc = bluestein_pre(x, in_rs, p->chirp[d], buf, n, m, nr, st);
+      if (!rc) rc = exec_device(p->inner[d], buf, m, buf, m, nr, 0, st);
+      if (!rc) rc = bluestein_post(buf, m, p->chirp[d], y, out_rs, n, nr, p->scale, st);
+    }
+  }
+  return rc;
+}
+
 // 2-D FFT on device pointers: two transposing row passes.
 int exec_2d(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs, cudaStream_t st)
 {
@@ -146,10 +241,11 @@ int exec_2d(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long lon
   return launch_rows(p->kc, p->cols2d, a, st);
 }
 
-// Device-pointer execution on stream st.
+// Device-pointer execution on stream st (slot: Bluestein work buffer).
 int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
-                long long rows, long long row0, cudaStream_t st)
+                long long rows, long long row0, cudaStream_t st, int slot)
 {
+  if (p->blue_m) return exec_blue(p, in, in_rs, out, out_rs, rows, row0, st, slot);
   const float4 *rep = p->rep ? p->rep + (p->rep_rows > 1 ? row0 * (p->n > 1 ? p->n / 2 : 1) : 0) : nullptr;
   long long rep_rs = p->rep_rows > 1 ? (p->n > 1 ? p->n / 2 : 1) : 0;
   if (p->logn == 0)
@@ -190,6 +286,11 @@ int ensure_staging(fcb_plan p, long long chunk_rows)
       if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
         return cuda_error(e, "cudaEventCreate");
   }
+  if (p->blue_m && !p->blue_buf[1])
+  {
+    cudaError_t e = cudaMalloc(&p->blue_buf[1], sizeof(float2) * (size_t)(p->blue_chunk * p->blue_m));
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "Bluestein work rows: %s", cudaGetErrorString(e));
+  }
   p->stage_rows = chunk_rows;
   return FCB_OK;
 }
@@ -217,7 +318,7 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
     cudaError_t e = cudaMemcpy2DAsync(buf, row_bytes, in + r0 * in_rs, sizeof(float2) * (size_t)in_rs,
                                       row_bytes, (size_t)nr, cudaMemcpyHostToDevice, st[i]);
     if (e != cudaSuccess) return cuda_error(e, "host->device copy");
-    rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, st[i]);
+    rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, st[i], i);
     if (rc) return rc;
     e = cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,
                           (size_t)nr, cudaMemcpyDeviceToHost, st[i]);
@@ -255,20 +356,23 @@ int fcb_init(int device)
 int fcb_supported_length(long long n)
 {
   int l = log2_exact(n);
-  return l >= 0 && l <= kMaxLogN;
+  return (l >= 0 && l <= kMaxLogN) || blue_length(n);
 }
 
 int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale, fcb_plan *plan)
 {
   if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
   *plan = nullptr;
-  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "row length %lld is not a power of two in [1, 65536]", n);
+  if (!fcb_supported_length(n))
+    return set_error(FCB_ERR_UNSUPPORTED, "row length %lld unsupported: " FCB_LENGTH_RULE, n);
   if (rows_max < 0) return set_error(FCB_ERR_INVALID, "rows_max < 0");
   if (exponent != FCB_FORWARD && exponent != FCB_INVERSE) return set_error(FCB_ERR_INVALID, "exponent must be -1 or +1");
   fcb_plan p = new (std::nothrow) fcb_plan_s;
   if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
   p->scale = scale;
-  int rc = plan_common(p, n, rows_max, exponent == FCB_FORWARD ? kFwd : kInv);
+  const int mode = exponent == FCB_FORWARD ? kFwd : kInv;
+  int rc = blue_length(n) ? blue_setup(p, n, rows_max, mode, mode == kFwd, mode == kInv)
+                          : plan_common(p, n, rows_max, mode);
   if (!rc)
   {
     cudaError_t e = cudaStreamSynchronize(p->stream);
@@ -284,7 +388,8 @@ int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, 
 {
   if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
   *plan = nullptr;
-  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "row length %lld is not a power of two in [1, 65536]", n);
+  if (!fcb_supported_length(n))
+    return set_error(FCB_ERR_UNSUPPORTED, "row length %lld unsupported: " FCB_LENGTH_RULE, n);
   if (!replica) return set_error(FCB_ERR_INVALID, "replica is NULL");
   if (replica_rows < 1) return set_error(FCB_ERR_INVALID, "replica_rows < 1");
   if (replica_rows > 1 && replica_rs < n) return set_error(FCB_ERR_INVALID, "replica row stride < n");
@@ -293,7 +398,8 @@ int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, 
   if (where != FCB_HOST && where != FCB_DEVICE) return set_error(FCB_ERR_INVALID, "bad location");
   fcb_plan p = new (std::nothrow) fcb_plan_s;
   if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
-  int rc = plan_common(p, n, rows_max, kFastconv);
+  const bool blue = blue_length(n);
+  int rc = blue ? blue_setup(p, n, rows_max, kFastconv, true, true) : plan_common(p, n, rows_max, kFastconv);
   float2 *spec = nullptr, *tmp = nullptr;
   if (!rc)
   {
@@ -316,7 +422,15 @@ int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, 
         rc = replica_spectrum_dev(spec + r * n, n, replica_kind == FCB_REPLICA_TIME_MATCHED, tmp + r * n, p->stream);
       if (!rc) std::swap(spec, tmp);
     }
-    if (!rc)
+    if (!rc && blue)
+    {
+      // R / n per row; 1/n is the inverse FFT's normalisation
+      p->rep_rows = replica_rows;
+      e = cudaMalloc(&p->blue_rep, bytes);
+      if (e != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "replica table: %s", cudaGetErrorString(e));
+      if (!rc) rc = scale_copy(spec, p->blue_rep, replica_rows * n, (float)(1.0 / (double)n), p->stream);
+    }
+    else if (!rc)
     {
       const long long slots = n > 1 ? n / 2 : 1;
       e = cudaMalloc(&p->rep, sizeof(float4) * (size_t)(replica_rows * slots));
@@ -424,10 +538,12 @@ int fcb_plan_info(fcb_plan p, long long *n, int *cluster_ctas, int *rows_per_cta
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
   if (n) *n = p->n;
-  if (threads) *threads = p->k ? p->k->threads : 0;
-  if (cluster_ctas) *cluster_ctas = p->k ? p->k->cluster : 1;
-  if (rows_per_cta) *rows_per_cta = p->k ? p->k->rows_per_cta : 1;
-  if (smem_bytes) *smem_bytes = p->k ? p->k->smem : 0;
+  // Bluestein plans report the kernel of their power-of-two work rows
+  const KernelInfo *k = p->k ? p->k : p->inner[0] ? p->inner[0]->k : p->inner[1] ? p->inner[1]->k : nullptr;
+  if (threads) *threads = k ? k->threads : 0;
+  if (cluster_ctas) *cluster_ctas = k ? k->cluster : 1;
+  if (rows_per_cta) *rows_per_cta = k ? k->rows_per_cta : 1;
+  if (smem_bytes) *smem_bytes = k ? k->smem : 0;
   return FCB_OK;
 }
 
@@ -500,7 +616,7 @@ int fcb_vmmul_rows(const fcb_cf32 *v, const fcb_cf32 *m, long long m_rs, fcb_cf3
 
 int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int matched, fcb_cf32 *spectrum_dev)
 {
-  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "length %lld is not a power of two in [1, 65536]", n);
+  if (!fcb_supported_length(n)) return set_error(FCB_ERR_UNSUPPORTED, "length %lld unsupported: " FCB_LENGTH_RULE, n);
   if (!replica_dev || !spectrum_dev) return set_error(FCB_ERR_INVALID, "NULL pointer");
   int rc = check_device();
   if (rc) return rc;

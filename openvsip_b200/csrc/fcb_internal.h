@@ -43,6 +43,17 @@ int launch_vmmul(const float2 *v, const float2 *m, long long m_rs, float2 *out, 
 int launch_scale_rows(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
                       const float4 *rep, long long rep_rs, float scale, cudaStream_t st);
 
+// Bluestein chirp-z pieces (fcb_bluestein.cu) for rows of non-power-of-two
+// length N, computed through power-of-two work rows of M >= 2N - 1 samples.
+int bluestein_tables(long long N, long long M, int sign, float2 **chirp, float2 **spectrum, cudaStream_t st);
+int bluestein_pre(const float2 *x, long long x_rs, const float2 *c, float2 *a, long long N, long long M,
+                  long long rows, cudaStream_t st);
+int bluestein_post(const float2 *y, long long M, const float2 *c, float2 *out, long long out_rs, long long N,
+                   long long rows, float scale, cudaStream_t st);
+int bluestein_mid(float2 *y, long long M, const float2 *rep, long long rep_rs, long long N, long long rows,
+                  cudaStream_t st);
+int scale_copy(const float2 *in, float2 *out, long long total, float s, cudaStream_t st);
+
 int set_error(int code, const char *fmt, ...);
 const char *error_text();
 int cuda_error(cudaError_t e, const char *what);

@@ -34,16 +34,18 @@ def test_every_export_is_declared():
 
 def test_supported_lengths():
     L = _lib.lib()
-    for n in (1, 2, 4, 1024, 65536):
+    # powers of two up to 65536 (one fused pass); any other length up to
+    # 32768 (Bluestein through power-of-two work rows of at most 65536)
+    for n in (1, 2, 3, 4, 18, 19, 68, 252, 768, 1024, 32767, 32768, 65536):
         assert L.fcb_supported_length(n) == 1
-    for n in (0, 3, 18, 768, 131072, -4):
+    for n in (0, 32769, 40000, 65535, 131072, -4):
         assert L.fcb_supported_length(n) == 0
 
 
 def test_argument_errors_without_device():
     L = _lib.lib()
     h = ctypes.c_void_p()
-    assert L.fcb_plan_fftm(768, 4, -1, 1.0, ctypes.byref(h)) == _lib.FCB_ERR_UNSUPPORTED
+    assert L.fcb_plan_fftm(40000, 4, -1, 1.0, ctypes.byref(h)) == _lib.FCB_ERR_UNSUPPORTED
     assert b"power of two" in L.fcb_last_error()
     assert L.fcb_plan_fftm(1024, 4, 0, 1.0, ctypes.byref(h)) == _lib.FCB_ERR_INVALID
     assert L.fcb_plan_fftm(1024, 4, -1, 1.0, None) == _lib.FCB_ERR_INVALID
