@@ -88,15 +88,26 @@ __global__ void build_tw_kernel(float4 *tw, SchedRT s)
   }
 }
 
-// Replica pair table in slot order: slot sigma = q'*D + P holds
-// (R[k]/N, R[k+1]/N) split, k = 2q' + R1 * digitrev16(P).  1/N is exact.
+// Replica pair table, (R[k]/N, R[k+1]/N) split per entry (1/N is exact).
+// Slot sigma = q'*D + P holds the pair k = 2q' + R1 * digitrev16(P).  Rows of
+// one stage keep slot order.  Multi-stage rows use the order in which the
+// last stage reads: there thread tr of a row (TPR = N/32 threads) owns slots
+// 16 tr .. 16 tr + 15 and multiplies its i-th value by slot 16 tr +
+// bitrev4(i), so entry i * TPR + tr holds that slot and the i-th loads of a
+// warp read consecutive entries (one coalesced 512-byte access).
 __global__ void build_rep_kernel(const float2 *spec, long long spec_rs, float4 *rep,
                                  long long rows, SchedRT s)
 {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long total = rows * s.half;
   if (i >= total) return;
-  long long r = i / s.half, sigma = i % s.half;
+  long long r = i / s.half, e = i % s.half;
+  long long sigma = e;
+  if (s.ns > 1)
+  {
+    const long long tpr = s.n / 32, j = e / tpr, tr = e % tpr;
+    sigma = 16 * tr + bitrev((int)j, 4);
+  }
   int qp = (int)(sigma / s.d), P = (int)(sigma % s.d);
   int k = 2 * qp + s.r1 * digitrev16(P, s.ns - 1);
   const float inv = 1.0f / (float)s.n;

@@ -29,7 +29,9 @@
 //    constant), because N = 32 T.
 //  * After the last forward stage a slot sigma = q'*D + P holds X[k], X[k+1]
 //    with k = 2q' + R1 * digitrev16(P).  The fused path multiplies by a replica
-//    table stored in that order (scaled by 1/N, exact for powers of two) and
+//    table stored in the order the last stage reads it (the i-th value of
+//    every thread of a row side by side, so each load is coalesced; scaled by
+//    1/N, exact for powers of two) and
 //    runs the exact transpose of the forward stages with conjugate twiddles, so
 //    no reordering pass is ever needed and every row makes one HBM read and one
 //    HBM write.  The standalone FFTs add one reorder exchange.
@@ -505,7 +507,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     if constexpr (MODE == kFastconv && s == S::NS)
     {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + base + St * bitrev(i, 4));
+      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + i * S::TPR + tr);
     }
     DifNet<16, SIGN>::run(c);
     if constexpr (St > 1)
@@ -527,7 +529,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 #pragma unroll
       for (int i = 0; i < 8; ++i) c[i] = cp_mul4(c[i], ra[i]);
 #pragma unroll
-      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + base + St * bitrev(8 + i, 4));
+      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + (8 + i) * S::TPR + tr);
 #pragma unroll
       for (int i = 0; i < 8; ++i) c[8 + i] = cp_mul4(c[8 + i], ra[i]);
     }
