@@ -318,6 +318,7 @@ struct RowArgs
   long long rep_rs;     // fused: replica row stride in slots (0 = one vector)
   float scale;          // standalone: output scale
   int transpose_out;    // standalone FFT: store the result transposed (2-D FFT passes)
+  int vec_out;          // standalone FFT: every output row starts 16-byte aligned
   long long ahead;      // L2 prefetch distance in tiles (CTAs, or clusters) -- about
                         // one resident wave, so that tile's rows stream from HBM
                         // into L2 while this tile computes; 0 = off
@@ -493,7 +494,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 
   // ---------------- stages 2..NS, direction SIGN ----------------
   // One radix-16 group per thread (CPT == 16 whenever NS > 1).  In the fused
-  // mode the last stage also multiplies by the replica (in two batches).
+  // mode the last stage also multiplies by the replica (four entries at a time).
   auto stage_fwd = [&](auto sc) {
     constexpr int s = decltype(sc)::value;
     constexpr int Lg = S::L(s), St = S::S(s);
@@ -503,35 +504,46 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 #pragma unroll
     for (int r = 0; r < 16; ++r)
       c[r] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * r, rho))));
-    float4 ra[8];
+    float4 ra[4];  // replica entries, four at a time
     if constexpr (MODE == kFastconv && s == S::NS)
     {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + i * S::TPR + tr);
+      for (int i = 0; i < 4; ++i) ra[i] = ldv4(rp + i * S::TPR + tr);
     }
     DifNet<16, SIGN>::run(c);
     if constexpr (St > 1)
     {
-      float2 w[16];
+      // twiddles in batches of four: fewer live registers (no spills)
 #pragma unroll
-      for (int q = 1; q < 16; ++q) w[q] = ld_tw(tw_base + 8u * (S::tw2_off(s) + q * St + n));
-#pragma unroll
-      for (int i = 0; i < 16; ++i)
+      for (int b = 0; b < 16; b += 4)
       {
-        const int q = bitrev(i, 4);
-        if (q != 0)
-          c[i] = (SIGN < 0) ? cp_mul<false>(c[i], f2dup(w[q].x), f2dup(w[q].y))
-                            : cp_mul<true>(c[i], f2dup(w[q].x), f2dup(w[q].y));
+        float2 w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (b + j > 0) w[j] = ld_tw(tw_base + 8u * (S::tw2_off(s) + (b + j) * St + n));
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+          const int q = b + j, i = bitrev(q, 4);
+          if (q != 0)
+            c[i] = (SIGN < 0) ? cp_mul<false>(c[i], f2dup(w[j].x), f2dup(w[j].y))
+                              : cp_mul<true>(c[i], f2dup(w[j].x), f2dup(w[j].y));
+        }
       }
     }
     if constexpr (MODE == kFastconv && s == S::NS)
     {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) c[i] = cp_mul4(c[i], ra[i]);
+      for (int b = 0; b < 16; b += 4)
+      {
+        if (b > 0)
+        {
 #pragma unroll
-      for (int i = 0; i < 8; ++i) ra[i] = ldv4(rp + (8 + i) * S::TPR + tr);
+          for (int i = 0; i < 4; ++i) ra[i] = ldv4(rp + (b + i) * S::TPR + tr);
+        }
 #pragma unroll
-      for (int i = 0; i < 8; ++i) c[8 + i] = cp_mul4(c[8 + i], ra[i]);
+        for (int i = 0; i < 4; ++i) c[b + i] = cp_mul4(c[b + i], ra[i]);
+      }
     }
     if constexpr (s < S::NS)
     {
@@ -616,8 +628,13 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       p.im = f2mul(p.im, sc);
       if (active)
       {
-        dstp[2 * m] = make_float2(p.re.x, p.im.x);
-        dstp[2 * m + 1] = make_float2(p.re.y, p.im.y);
+        if (a.vec_out)  // one 16-byte store per pair (row start 16-byte aligned)
+          reinterpret_cast<float4 *>(dstp)[m] = make_float4(p.re.x, p.im.x, p.re.y, p.im.y);
+        else
+        {
+          dstp[2 * m] = make_float2(p.re.x, p.im.x);
+          dstp[2 * m + 1] = make_float2(p.re.y, p.im.y);
+        }
       }
     }
     return;
@@ -660,11 +677,17 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       }
       if constexpr (St > 1)
       {
-        float2 w[16];
 #pragma unroll
-        for (int q = 1; q < 16; ++q) w[q] = ld_tw(tw_base + 8u * (S::tw2_off(s) + q * St + n));
+        for (int b = 0; b < 16; b += 4)
+        {
+          float2 w[4];
 #pragma unroll
-        for (int q = 1; q < 16; ++q) z[q] = cp_mul<true>(z[q], f2dup(w[q].x), f2dup(w[q].y));
+          for (int j = 0; j < 4; ++j)
+            if (b + j > 0) w[j] = ld_tw(tw_base + 8u * (S::tw2_off(s) + (b + j) * St + n));
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (b + j > 0) z[b + j] = cp_mul<true>(z[b + j], f2dup(w[j].x), f2dup(w[j].y));
+        }
       }
       DifNet<16, +1>::run(z);  // z[i] = y[bitrev(i)]
 #pragma unroll
@@ -687,7 +710,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     }
 
     // ---------------- inverse stage 1 and store ----------------
-    float2 *dstp = a.out + row * a.out_rs;
+    float2 *dst_t = a.out + row * a.out_rs + tr;  // outputs at constant offsets from here
     // all slot reads of this thread first (remote ones in a cluster have a long
     // round trip; issuing them together overlaps their latencies)
     float4 v[S::CPT];
@@ -734,8 +757,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         else { tr_ = fmaf(br, wc, -bi * ws); ti_ = fmaf(br, ws, bi * wc); }
         if (active)
         {
-          dstp[n + S::D * r] = make_float2(ar + tr_, ai + ti_);
-          dstp[n + S::D * (r + S::H1)] = make_float2(ar - tr_, ai - ti_);
+          dst_t[S::TPR * g + S::D * r] = make_float2(ar + tr_, ai + ti_);
+          dst_t[S::TPR * g + S::D * (r + S::H1)] = make_float2(ar - tr_, ai - ti_);
         }
       }
     }
