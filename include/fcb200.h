@@ -105,6 +105,28 @@ FCB_API int fcb_supported_length(long long n);
 FCB_API int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale,
                   fcb_plan *plan);
 
+/* Real-input row FFTs.  exponent FCB_FORWARD: real rows of n samples ->
+ * complex rows of n/2 + 1 (the non-negative frequencies), run with
+ * fcb_exec_r2c; FCB_INVERSE: complex rows of n/2 + 1 -> real rows of n,
+ * unnormalised like FFTW's c2r (imaginary parts of bins 0 and n/2 ignored),
+ * run with fcb_exec_c2r.  Output times scale.  Replaces
+ * fftm_backend<float, complex<float>, A, fft_fwd> and
+ * fftm_backend<complex<float>, float, A, fft_inv> (src/ovxx/signal/fft/
+ * backend.hpp:600-694; FFTW rows src/ovxx/fftw/fftw.cpp:778-903).  Even n:
+ * one length-n/2 complex row FFT plus a split (forward) or merge (inverse)
+ * pass; odd n: the length-n complex row FFT. */
+FCB_API int fcb_supported_real_length(long long n);
+FCB_API int fcb_plan_fftm_real(long long n, long long rows_max, int exponent, float scale,
+                               fcb_plan *plan);
+/* in: rows of n floats (stride in_rs floats); out: rows of n/2 + 1 complex
+ * (stride out_rs complex).  in and out must not overlap.  where as fcb_exec. */
+FCB_API int fcb_exec_r2c(fcb_plan plan, const float *in, long long in_rs, fcb_cf32 *out,
+                         long long out_rs, long long rows, int where);
+/* in: rows of n/2 + 1 complex (stride in_rs complex); out: rows of n floats
+ * (stride out_rs floats).  in and out must not overlap. */
+FCB_API int fcb_exec_c2r(fcb_plan plan, const fcb_cf32 *in, long long in_rs, float *out,
+                         long long out_rs, long long rows, int where);
+
 /* 2-D FFT plan over a rows x cols matrix (both powers of two in [64, 16384]),
  * output times scale; fcb_exec then takes rows == the plan's rows.  Replaces
  * fft_backend<2, complex<float>, complex<float>, S> (src/ovxx/signal/fft/

@@ -7,6 +7,7 @@ the synthetic workload generators.
 """
 from ._lib import FcbError, lib  # noqa: F401
 from . import synth  # noqa: F401
-from .vsip import Fastconv, Fft2d, Fftm, fft_fwd, fft_inv, replica_spectrum, supported_length, vmmul  # noqa: F401
+from .vsip import (Fastconv, Fft2d, Fftm, FftmReal, col, fft_fwd, fft_inv, replica_spectrum, row,  # noqa: F401
+                   supported_length, vmmul)
 
 __version__ = "0.1.0"

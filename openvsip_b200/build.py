@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 
-SOURCES = ["fcb200.cu", "fcb_api.cu", "fcb_batch.cu", "fcb_bluestein.cu"]
+SOURCES = ["fcb200.cu", "fcb_api.cu", "fcb_batch.cu", "fcb_bluestein.cu", "fcb_real.cu"]
 
 
 def nvcc() -> str:

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <new>
 
 using namespace fcb;
@@ -45,6 +46,17 @@ struct fcb_plan_s
   fcb_plan inner[2] = {nullptr, nullptr};      // length-blue_m fastconv, replica FFT(conj(c))
   float2 *blue_rep = nullptr;                  // fastconv: replica spectra / n, rows of n
   float2 *blue_buf[2] = {nullptr, nullptr};    // work rows, one per staging stream
+  // Real-input rows of n = rn samples: 1 = real -> complex (n/2 + 1 outputs),
+  // 2 = complex -> real.  Even n: a length-n/2 complex plan plus the split /
+  // merge step; odd n: a length-n complex plan on expanded rows.
+  int real = 0;
+  long long rn = 0;
+  fcb_plan cplx = nullptr;
+  float2 *rtw = nullptr;               // W_n^k, k = 0 .. n/2 (even n)
+  float2 *rbuf = nullptr;              // work rows (odd n, or unaligned rows)
+  long long rbuf_rows = 0, rbuf_cols = 0;
+  void *rstage[2] = {nullptr, nullptr};  // host calls: device copies of in / out
+  long long rstage_rows = 0;
 };
 
 namespace {
@@ -116,6 +128,11 @@ void plan_free(fcb_plan p)
     cudaFree(p->blue_buf[d]);
   }
   cudaFree(p->blue_rep);
+  plan_free(p->cplx);
+  cudaFree(p->rtw);
+  cudaFree(p->rbuf);
+  cudaFree(p->rstage[0]);
+  cudaFree(p->rstage[1]);
   for (auto &e : p->done) if (e) cudaEventDestroy(e);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
   if (p->aux) cudaStreamDestroy(p->aux);
@@ -214,6 +231,170 @@ int exec_blue(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
     }
   }
   return rc;
+}
+
+bool aligned8(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 7) == 0; }
+
+int ensure_rbuf(fcb_plan p, long long cols)
+{
+  if (p->rbuf) return FCB_OK;
+  p->rbuf_cols = cols;
+  p->rbuf_rows = std::max<long long>(1, std::min<long long>(std::max<long long>(p->rows_max, 1), (1LL << 24) / cols));
+  cudaError_t e = cudaMalloc(&p->rbuf, sizeof(float2) * (size_t)(p->rbuf_rows * cols));
+  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "real-FFT work rows: %s", cudaGetErrorString(e));
+  return FCB_OK;
+}
+
+// Real-input rows on device pointers, stream st.  in / out: float rows of n
+// (real side) or complex rows of n/2 + 1 (spectrum side); strides in elements.
+int exec_real_device(fcb_plan p, const void *in, long long in_rs, void *out, long long out_rs, long long rows,
+                     cudaStream_t st)
+{
+  const long long n = p->rn;
+  int rc = FCB_OK;
+  if (n % 2 == 0)
+  {
+    const long long m = n / 2;
+    if (p->real == 1)
+    {
+      const float *x = static_cast<const float *>(in);
+      float2 *y = static_cast<float2 *>(out);
+      const bool direct = aligned8(x) && (in_rs % 2 == 0 || rows == 1);
+      if (!direct && (rc = ensure_rbuf(p, m))) return rc;
+      const long long chunk = direct ? rows : p->rbuf_rows;
+      for (long long r0 = 0; !rc && r0 < rows; r0 += chunk)
+      {
+        const long long nr = std::min(chunk, rows - r0);
+        const float2 *z = reinterpret_cast<const float2 *>(x + r0 * in_rs);
+        long long z_rs = rows == 1 ? m : in_rs / 2;
+        if (!direct)
+        {
+          cudaError_t e = cudaMemcpy2DAsync(p->rbuf, sizeof(float2) * (size_t)m, x + r0 * in_rs,
+                                            sizeof(float) * (size_t)in_rs, sizeof(float) * (size_t)n, (size_t)nr,
+                                            cudaMemcpyDeviceToDevice, st);
+          if (e != cudaSuccess) return cuda_error(e, "real rows copy");
+          z = p->rbuf;
+          z_rs = m;
+        }
+        rc = exec_device(p->cplx, z, z_rs, y + r0 * out_rs, out_rs, nr, 0, st);
+        if (!rc) rc = r2c_post(y + r0 * out_rs, out_rs, m, nr, p->rtw, p->scale, st);
+      }
+    }
+    else
+    {
+      const float2 *x = static_cast<const float2 *>(in);
+      float *y = static_cast<float *>(out);
+      const bool direct = aligned8(y) && (out_rs % 2 == 0 || rows == 1);
+      if (!direct && (rc = ensure_rbuf(p, m))) return rc;
+      const long long chunk = direct ? rows : p->rbuf_rows;
+      for (long long r0 = 0; !rc && r0 < rows; r0 += chunk)
+      {
+        const long long nr = std::min(chunk, rows - r0);
+        float2 *z = direct ? reinterpret_cast<float2 *>(y + r0 * out_rs) : p->rbuf;
+        const long long z_rs = direct ? (rows == 1 ? m : out_rs / 2) : m;
+        rc = c2r_pre(x + r0 * in_rs, in_rs, z, z_rs, m, nr, p->rtw, st);
+        if (!rc) rc = exec_device(p->cplx, z, z_rs, z, z_rs, nr, 0, st);
+        if (!rc && !direct)
+        {
+          cudaError_t e = cudaMemcpy2DAsync(y + r0 * out_rs, sizeof(float) * (size_t)out_rs, p->rbuf,
+                                            sizeof(float2) * (size_t)m, sizeof(float) * (size_t)n, (size_t)nr,
+                                            cudaMemcpyDeviceToDevice, st);
+          if (e != cudaSuccess) return cuda_error(e, "real rows copy");
+        }
+      }
+    }
+    return rc;
+  }
+  // odd n: through full-length complex rows
+  if ((rc = ensure_rbuf(p, n))) return rc;
+  for (long long r0 = 0; !rc && r0 < rows; r0 += p->rbuf_rows)
+  {
+    const long long nr = std::min(p->rbuf_rows, rows - r0);
+    if (p->real == 1)
+    {
+      const float *x = static_cast<const float *>(in) + r0 * in_rs;
+      float2 *y = static_cast<float2 *>(out) + r0 * out_rs;
+      rc = real_expand(x, in_rs, p->rbuf, n, nr, st);
+      if (!rc) rc = exec_device(p->cplx, p->rbuf, n, p->rbuf, n, nr, 0, st);
+      if (!rc)
+      {
+        cudaError_t e = cudaMemcpy2DAsync(y, sizeof(float2) * (size_t)out_rs, p->rbuf, sizeof(float2) * (size_t)n,
+                                          sizeof(float2) * (size_t)(n / 2 + 1), (size_t)nr,
+                                          cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) rc = cuda_error(e, "half-spectrum copy");
+      }
+    }
+    else
+    {
+      const float2 *x = static_cast<const float2 *>(in) + r0 * in_rs;
+      float *y = static_cast<float *>(out) + r0 * out_rs;
+      rc = herm_expand(x, in_rs, p->rbuf, n, nr, st);
+      if (!rc) rc = exec_device(p->cplx, p->rbuf, n, p->rbuf, n, nr, 0, st);
+      if (!rc) rc = take_real(p->rbuf, n, y, out_rs, nr, st);
+    }
+  }
+  return rc;
+}
+
+// Real-input rows on host pointers: chunks staged through two device buffers.
+int exec_real_host(fcb_plan p, const void *in, long long in_rs, void *out, long long out_rs, long long rows)
+{
+  const long long n = p->rn, h = n / 2 + 1;
+  const size_t in_el = p->real == 1 ? sizeof(float) : sizeof(float2);
+  const size_t out_el = p->real == 1 ? sizeof(float2) : sizeof(float);
+  const long long in_cols = p->real == 1 ? n : h, out_cols = p->real == 1 ? h : n;
+  // even column counts keep every staged row 8-byte aligned
+  const long long in_pitch = in_cols + (in_cols & 1), out_pitch = out_cols + (out_cols & 1);
+  const long long row_bytes = (long long)(in_el * in_pitch + out_el * out_pitch);
+  const long long chunk = std::min(rows, std::max<long long>(1, (32LL << 20) / row_bytes));
+  if (p->rstage_rows < chunk)
+  {
+    cudaFree(p->rstage[0]);
+    cudaFree(p->rstage[1]);
+    p->rstage[0] = p->rstage[1] = nullptr;
+    p->rstage_rows = 0;
+    cudaError_t e = cudaMalloc(&p->rstage[0], in_el * (size_t)(chunk * in_pitch));
+    if (e == cudaSuccess) e = cudaMalloc(&p->rstage[1], out_el * (size_t)(chunk * out_pitch));
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "staging buffer: %s", cudaGetErrorString(e));
+    p->rstage_rows = chunk;
+  }
+  const char *src = static_cast<const char *>(in);
+  char *dst = static_cast<char *>(out);
+  for (long long r0 = 0; r0 < rows; r0 += chunk)
+  {
+    const long long nr = std::min(chunk, rows - r0);
+    cudaError_t e = cudaMemcpy2DAsync(p->rstage[0], in_el * (size_t)in_pitch, src + in_el * (size_t)(r0 * in_rs),
+                                      in_el * (size_t)in_rs, in_el * (size_t)in_cols, (size_t)nr,
+                                      cudaMemcpyHostToDevice, p->stream);
+    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    int rc = exec_real_device(p, p->rstage[0], in_pitch, p->rstage[1], out_pitch, nr, p->stream);
+    if (rc) return rc;
+    e = cudaMemcpy2DAsync(dst + out_el * (size_t)(r0 * out_rs), out_el * (size_t)out_rs, p->rstage[1],
+                          out_el * (size_t)out_pitch, out_el * (size_t)out_cols, (size_t)nr,
+                          cudaMemcpyDeviceToHost, p->stream);
+    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+  }
+  cudaError_t e = cudaStreamSynchronize(p->stream);
+  return e == cudaSuccess ? FCB_OK : cuda_error(e, "real FFT (host)");
+}
+
+int exec_real(fcb_plan p, int kind, const void *in, long long in_rs, void *out, long long out_rs, long long rows,
+              int where)
+{
+  if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
+  if (p->real != kind)
+    return set_error(FCB_ERR_INVALID, p->real ? "wrong direction for this real-FFT plan"
+                                              : "not a real-FFT plan (use fcb_exec)");
+  if (rows < 0 || rows > p->rows_max) return set_error(FCB_ERR_INVALID, "rows %lld outside [0, %lld]", rows, p->rows_max);
+  if (rows == 0) return FCB_OK;
+  if (!in || !out) return set_error(FCB_ERR_INVALID, "NULL data pointer");
+  const long long h = p->rn / 2 + 1;
+  const long long in_min = kind == 1 ? p->rn : h, out_min = kind == 1 ? h : p->rn;
+  if (in_rs < in_min || out_rs < out_min) return set_error(FCB_ERR_INVALID, "row stride smaller than the row length");
+  if (where != FCB_HOST && where != FCB_DEVICE) return set_error(FCB_ERR_INVALID, "bad location");
+  DeviceGuard g(p->device);
+  if (where == FCB_DEVICE) return exec_real_device(p, in, in_rs, out, out_rs, rows, p->stream);
+  return exec_real_host(p, in, in_rs, out, out_rs, rows);
 }
 
 // 2-D FFT on device pointers: two transposing row passes.
@@ -472,6 +653,7 @@ int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, lon
              long long rows, int where)
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
+  if (p->real) return set_error(FCB_ERR_INVALID, "real-FFT plans run through fcb_exec_r2c / fcb_exec_c2r");
   if (rows < 0 || rows > p->rows_max) return set_error(FCB_ERR_INVALID, "rows %lld outside [0, %lld]", rows, p->rows_max);
   if (p->mode == kFastconv && p->rep_rows > 1 && rows > p->rep_rows)
     return set_error(FCB_ERR_INVALID, "rows %lld exceed the replica matrix rows %lld", rows, p->rep_rows);
@@ -539,13 +721,67 @@ int fcb_plan_info(fcb_plan p, long long *n, int *cluster_ctas, int *rows_per_cta
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
   if (n) *n = p->n;
-  // Bluestein plans report the kernel of their power-of-two work rows
-  const KernelInfo *k = p->k ? p->k : p->inner[0] ? p->inner[0]->k : p->inner[1] ? p->inner[1]->k : nullptr;
+  // Bluestein and real-input plans report the kernel of their power-of-two work rows
+  fcb_plan q = p->cplx ? p->cplx : p;
+  const KernelInfo *k = q->k ? q->k : q->inner[0] ? q->inner[0]->k : q->inner[1] ? q->inner[1]->k : nullptr;
   if (threads) *threads = k ? k->threads : 0;
   if (cluster_ctas) *cluster_ctas = k ? k->cluster : 1;
   if (rows_per_cta) *rows_per_cta = k ? k->rows_per_cta : 1;
   if (smem_bytes) *smem_bytes = k ? k->smem : 0;
   return FCB_OK;
+}
+
+int fcb_supported_real_length(long long n)
+{
+  if (n < 1) return 0;
+  return n % 2 == 0 ? fcb_supported_length(n / 2) : fcb_supported_length(n);
+}
+
+int fcb_plan_fftm_real(long long n, long long rows_max, int exponent, float scale, fcb_plan *plan)
+{
+  if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
+  *plan = nullptr;
+  if (!fcb_supported_real_length(n))
+    return set_error(FCB_ERR_UNSUPPORTED, "real row length %lld unsupported: even with n/2 " FCB_LENGTH_RULE
+                     ", or odd up to 32767", n);
+  if (rows_max < 0) return set_error(FCB_ERR_INVALID, "rows_max < 0");
+  if (exponent != FCB_FORWARD && exponent != FCB_INVERSE) return set_error(FCB_ERR_INVALID, "exponent must be -1 or +1");
+  int rc = check_device();
+  if (rc) return rc;
+  fcb_plan p = new (std::nothrow) fcb_plan_s;
+  if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
+  cudaGetDevice(&p->device);
+  p->real = exponent == FCB_FORWARD ? 1 : 2;
+  p->rn = n;
+  p->n = n;
+  p->logn = -1;
+  p->mode = exponent == FCB_FORWARD ? kFwd : kInv;
+  p->rows_max = rows_max;
+  p->scale = scale;
+  cudaError_t e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamCreate");
+  p->stream = p->own_stream;
+  const bool even = n % 2 == 0;
+  if (!rc)
+    rc = fcb_plan_fftm(even ? n / 2 : n, std::max<long long>(rows_max, 1), exponent,
+                       (even && p->real == 1) ? 1.f : scale, &p->cplx);
+  if (!rc && even) rc = real_twiddles(n, n / 2 + 1, &p->rtw, p->stream);
+  if (!rc && (e = cudaStreamSynchronize(p->stream)) != cudaSuccess) rc = cuda_error(e, "real-FFT tables");
+  if (rc) { plan_free(p); return rc; }
+  *plan = p;
+  return FCB_OK;
+}
+
+int fcb_exec_r2c(fcb_plan p, const float *in, long long in_rs, fcb_cf32 *out, long long out_rs, long long rows,
+                 int where)
+{
+  return exec_real(p, 1, in, in_rs, out, out_rs, rows, where);
+}
+
+int fcb_exec_c2r(fcb_plan p, const fcb_cf32 *in, long long in_rs, float *out, long long out_rs, long long rows,
+                 int where)
+{
+  return exec_real(p, 2, in, in_rs, out, out_rs, rows, where);
 }
 
 int fcb_plan_fft2d(long long rows, long long cols, int exponent, float scale, fcb_plan *plan)

@@ -54,6 +54,15 @@ int bluestein_mid(float2 *y, long long M, const float2 *rep, long long rep_rs, l
                   cudaStream_t st);
 int scale_copy(const float2 *in, float2 *out, long long total, float s, cudaStream_t st);
 
+// Real-input row FFTs (fcb_real.cu).
+int real_twiddles(long long n, long long count, float2 **out, cudaStream_t st);
+int r2c_post(float2 *y, long long rs, long long m, long long rows, const float2 *w, float scale, cudaStream_t st);
+int c2r_pre(const float2 *x, long long x_rs, float2 *z, long long z_rs, long long m, long long rows,
+            const float2 *w, cudaStream_t st);
+int real_expand(const float *x, long long x_rs, float2 *z, long long n, long long rows, cudaStream_t st);
+int herm_expand(const float2 *x, long long x_rs, float2 *z, long long n, long long rows, cudaStream_t st);
+int take_real(const float2 *z, long long n, float *out, long long out_rs, long long rows, cudaStream_t st);
+
 int set_error(int code, const char *fmt, ...);
 const char *error_text();
 int cuda_error(cudaError_t e, const char *what);

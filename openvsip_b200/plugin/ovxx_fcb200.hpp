@@ -4,18 +4,21 @@
 // No reference header is modified: the plugin fills two dispatch slots the
 // reference already reserves.
 //
-//  1. be::user for op::fftm<complex<float>, complex<float>, row, D, R, N>.
-//     be::user is the first entry of List<op::fftm> (src/ovxx/signal/fft.hpp:
-//     57-64), so every row-wise complex<float> vsip::Fftm whose length the
-//     backend supports (powers of two up to 65536) is built on the B200.  The
-//     backend object follows the fftm_backend contract
-//     (src/ovxx/signal/fft/backend.hpp:696-784): it asks the DDA layer for
-//     dense, row-major, interleaved data (anything else is copied by
-//     dda::Rt_data before the call) and applies the scale itself
-//     (supports_scale() == true), so the workspace's separate scale pass
-//     (src/ovxx/signal/fft/workspace.hpp:474-478) is skipped.  Lengths the
-//     backend does not support fail rt_valid() and the dispatcher moves on to
-//     the next backend in the list, exactly as for any other plugin.
+//  1. be::user for op::fftm<complex<float>, complex<float>, row | col, D, R, N>
+//     and for the real-input forms op::fftm<float, complex<float>, A, fft_fwd>
+//     and op::fftm<complex<float>, float, A, fft_inv>.  be::user is the first
+//     entry of List<op::fftm> (src/ovxx/signal/fft.hpp:57-64), so every
+//     complex<float> / float vsip::Fftm whose length the backend supports (any
+//     length up to 32768, powers of two up to 65536; twice that for the real
+//     forms) is built on the B200.  The backend objects follow the fftm_backend
+//     contract (src/ovxx/signal/fft/backend.hpp:600-784): they ask the DDA
+//     layer for dense, interleaved data with unit stride along the transform
+//     axis (anything else, split storage included, is copied by dda::Rt_data
+//     before the call) and apply the scale themselves (supports_scale() ==
+//     true), so the workspace's separate scale pass (src/ovxx/signal/fft/
+//     workspace.hpp:474-478) is skipped.  Lengths the backend does not support
+//     fail rt_valid() and the dispatcher moves on to the next backend in the
+//     list, exactly as for any other plugin.
 //
 //  2. be::fc_expr for op::assign<2>, the "fused fastconv" slot that the
 //     reference lists (src/ovxx/assign_fwd.hpp:58, src/ovxx/dispatcher/
@@ -187,6 +190,151 @@ private:
   float fused_scale_;
 };
 
+/// fftm_backend for column-wise complex<float> multiple FFTs (Fftm<C, C, col,
+/// D>).  query_layout asks for column-major dense data (tuple<1,0,2>), so the
+/// DDA layer hands every column over as one contiguous run -- the layout the
+/// reference's FFTW backend requests for this axis (src/ovxx/fftw/fftw.cpp:
+/// 920-932) -- and the columns run as rows of the B200 row kernel.
+template <int D>
+class fftm_col : public signal::fft::fftm_backend<ctype, ctype, 1, D>
+{
+public:
+  fftm_col(Domain<2> const &dom, float scale) : n_(dom[0].size()), plan_(0)
+  {
+    ensure_device();
+    check(fcb_plan_fftm((long long)n_, (long long)dom[1].size(), D == fft_fwd ? FCB_FORWARD : FCB_INVERSE,
+                        scale, &plan_));
+    if (trace())
+      std::fprintf(stderr, "[fcb200] Fftm<%s, col> %lu x %lu scale %g on the B200\n",
+                   D == fft_fwd ? "fwd" : "inv", (unsigned long)n_, (unsigned long)dom[1].size(), (double)scale);
+  }
+  ~fftm_col() { if (plan_) fcb_destroy(plan_); }
+  virtual char const *name() { return "fcb200::fftm_col"; }
+  virtual bool supports_scale() { return true; }
+  virtual void query_layout(Rt_layout<2> &inout)
+  {
+    inout.packing = dense;
+    inout.order = tuple<1, 0, 2>();
+    inout.storage_format = array;
+  }
+  virtual void query_layout(Rt_layout<2> &in, Rt_layout<2> &out)
+  {
+    query_layout(in);
+    out = in;
+  }
+  virtual bool requires_copy(Rt_layout<2> &) { return false; }
+  virtual void in_place(ctype *inout, stride_type r, stride_type c, length_type rows, length_type cols)
+  {
+    run(inout, r, c, inout, r, c, rows, cols);
+  }
+  virtual void out_of_place(ctype *in, stride_type ir, stride_type ic, ctype *out, stride_type o_r,
+                            stride_type oc, length_type rows, length_type cols)
+  {
+    run(in, ir, ic, out, o_r, oc, rows, cols);
+  }
+
+private:
+  void run(ctype *in, stride_type ir, stride_type ic, ctype *out, stride_type o_r, stride_type oc,
+           length_type rows, length_type cols)
+  {
+    OVXX_PRECONDITION(ir == 1 && o_r == 1 && rows == n_);
+    if (cols == 0) return;
+    check(fcb_exec(plan_, reinterpret_cast<fcb_cf32 const *>(in), cols > 1 ? ic : rows,
+                   reinterpret_cast<fcb_cf32 *>(out), cols > 1 ? oc : rows, (long long)cols, FCB_HOST));
+  }
+
+  length_type n_;
+  fcb_plan plan_;
+};
+
+/// Layout of the real-input backends: unit stride along the transform axis
+/// (rows for A == row, columns for A == col), interleaved complex.
+template <int A>
+inline void real_layout(Rt_layout<2> &in, Rt_layout<2> &out)
+{
+  in.packing = out.packing = dense;
+  if (A == vsip::col) in.order = tuple<1, 0, 2>();
+  else in.order = tuple<0, 1, 2>();
+  out.order = in.order;
+  in.storage_format = out.storage_format = array;
+}
+
+/// fftm_backend for real -> complex multiple FFTs (Fftm<float, complex<float>,
+/// A, fft_fwd>): n real samples in, n/2 + 1 bins out, along rows (A == row) or
+/// columns (A == col).  The reference's own backends leave the scale to the
+/// workspace; this one folds it into the transform.
+template <int A>
+class fftm_r2c : public signal::fft::fftm_backend<float, ctype, A, fft_fwd>
+{
+  static int const axis = A == vsip::col ? 0 : 1;
+
+public:
+  fftm_r2c(Domain<2> const &dom, float scale) : n_(dom[axis].size()), plan_(0)
+  {
+    ensure_device();
+    check(fcb_plan_fftm_real((long long)n_, (long long)dom[1 - axis].size(), FCB_FORWARD, scale, &plan_));
+    if (trace())
+      std::fprintf(stderr, "[fcb200] Fftm<real->complex, %s> n %lu x %lu scale %g on the B200\n",
+                   axis == 1 ? "row" : "col", (unsigned long)n_, (unsigned long)dom[1 - axis].size(), (double)scale);
+  }
+  ~fftm_r2c() { if (plan_) fcb_destroy(plan_); }
+  virtual char const *name() { return "fcb200::fftm_r2c"; }
+  virtual bool supports_scale() { return true; }
+  virtual void query_layout(Rt_layout<2> &in, Rt_layout<2> &out) { real_layout<A>(in, out); }
+  virtual bool requires_copy(Rt_layout<2> &) { return false; }
+  virtual void out_of_place(float *in, stride_type i0, stride_type i1, ctype *out, stride_type o0, stride_type o1,
+                            length_type rows, length_type cols)
+  {
+    length_type const mult = axis == 1 ? rows : cols;
+    stride_type const in_rs = axis == 1 ? i0 : i1, out_rs = axis == 1 ? o0 : o1;
+    OVXX_PRECONDITION((axis == 1 ? i1 : i0) == 1 && (axis == 1 ? o1 : o0) == 1);
+    if (mult == 0) return;
+    check(fcb_exec_r2c(plan_, in, mult > 1 ? in_rs : n_, reinterpret_cast<fcb_cf32 *>(out),
+                       mult > 1 ? out_rs : n_ / 2 + 1, (long long)mult, FCB_HOST));
+  }
+
+private:
+  length_type n_;
+  fcb_plan plan_;
+};
+
+/// fftm_backend for complex -> real multiple FFTs (Fftm<complex<float>, float,
+/// A, fft_inv>): n/2 + 1 bins in, n real samples out.
+template <int A>
+class fftm_c2r : public signal::fft::fftm_backend<ctype, float, A, fft_inv>
+{
+  static int const axis = A == vsip::col ? 0 : 1;
+
+public:
+  fftm_c2r(Domain<2> const &dom, float scale) : n_(dom[axis].size()), plan_(0)
+  {
+    ensure_device();
+    check(fcb_plan_fftm_real((long long)n_, (long long)dom[1 - axis].size(), FCB_INVERSE, scale, &plan_));
+    if (trace())
+      std::fprintf(stderr, "[fcb200] Fftm<complex->real, %s> n %lu x %lu scale %g on the B200\n",
+                   axis == 1 ? "row" : "col", (unsigned long)n_, (unsigned long)dom[1 - axis].size(), (double)scale);
+  }
+  ~fftm_c2r() { if (plan_) fcb_destroy(plan_); }
+  virtual char const *name() { return "fcb200::fftm_c2r"; }
+  virtual bool supports_scale() { return true; }
+  virtual void query_layout(Rt_layout<2> &in, Rt_layout<2> &out) { real_layout<A>(in, out); }
+  virtual bool requires_copy(Rt_layout<2> &) { return false; }
+  virtual void out_of_place(ctype *in, stride_type i0, stride_type i1, float *out, stride_type o0, stride_type o1,
+                            length_type rows, length_type cols)
+  {
+    length_type const mult = axis == 1 ? rows : cols;
+    stride_type const in_rs = axis == 1 ? i0 : i1, out_rs = axis == 1 ? o0 : o1;
+    OVXX_PRECONDITION((axis == 1 ? i1 : i0) == 1 && (axis == 1 ? o1 : o0) == 1);
+    if (mult == 0) return;
+    check(fcb_exec_c2r(plan_, reinterpret_cast<fcb_cf32 const *>(in), mult > 1 ? in_rs : n_ / 2 + 1, out,
+                       mult > 1 ? out_rs : n_, (long long)mult, FCB_HOST));
+  }
+
+private:
+  length_type n_;
+  fcb_plan plan_;
+};
+
 // Fused plan for a weights block: a vector (one replica spectrum for all rows)
 // or a matrix (one per row), read through the DDA layer (direct pointer when
 // the block is dense, a copy otherwise).
@@ -259,6 +407,65 @@ struct Evaluator<op::fftm<std::complex<float>, std::complex<float>, 0, D, R, N>,
   static std::unique_ptr<backend_type> exec(Domain<2> const &dom, float scale)
   {
     return std::unique_ptr<backend_type>(new fcb200::fftm<D>(dom, scale));
+  }
+};
+
+/// Column-wise complex<float> Fftm on the B200 (be::user slot).
+template <int D, vsip::return_mechanism_type R, unsigned N>
+struct Evaluator<op::fftm<std::complex<float>, std::complex<float>, 1, D, R, N>, be::user,
+                 std::unique_ptr<signal::fft::fftm_backend<std::complex<float>, std::complex<float>, 1, D> >
+                 (Domain<2> const &, float)>
+{
+  typedef signal::fft::fftm_backend<std::complex<float>, std::complex<float>, 1, D> backend_type;
+  static bool const ct_valid = true;
+  static char const *name() { return "fcb200 fftm, columns (B200)"; }
+  static bool rt_valid(Domain<2> const &dom, float)
+  {
+    return fcb_supported_length((long long)dom[0].size()) && dom[1].size() > 0;
+  }
+  static std::unique_ptr<backend_type> exec(Domain<2> const &dom, float scale)
+  {
+    return std::unique_ptr<backend_type>(new fcb200::fftm_col<D>(dom, scale));
+  }
+};
+
+/// Real -> complex Fftm, rows or columns (be::user slot).
+template <int A, vsip::return_mechanism_type R, unsigned N>
+struct Evaluator<op::fftm<float, std::complex<float>, A, fft_fwd, R, N>, be::user,
+                 std::unique_ptr<signal::fft::fftm_backend<float, std::complex<float>, A, fft_fwd> >
+                 (Domain<2> const &, float)>
+{
+  typedef signal::fft::fftm_backend<float, std::complex<float>, A, fft_fwd> backend_type;
+  static bool const ct_valid = true;
+  static char const *name() { return "fcb200 fftm real->complex (B200)"; }
+  static bool rt_valid(Domain<2> const &dom, float)
+  {
+    int const axis = A == vsip::col ? 0 : 1;
+    return fcb_supported_real_length((long long)dom[axis].size()) && dom[1 - axis].size() > 0;
+  }
+  static std::unique_ptr<backend_type> exec(Domain<2> const &dom, float scale)
+  {
+    return std::unique_ptr<backend_type>(new fcb200::fftm_r2c<A>(dom, scale));
+  }
+};
+
+/// Complex -> real Fftm, rows or columns (be::user slot).
+template <int A, vsip::return_mechanism_type R, unsigned N>
+struct Evaluator<op::fftm<std::complex<float>, float, A, fft_inv, R, N>, be::user,
+                 std::unique_ptr<signal::fft::fftm_backend<std::complex<float>, float, A, fft_inv> >
+                 (Domain<2> const &, float)>
+{
+  typedef signal::fft::fftm_backend<std::complex<float>, float, A, fft_inv> backend_type;
+  static bool const ct_valid = true;
+  static char const *name() { return "fcb200 fftm complex->real (B200)"; }
+  static bool rt_valid(Domain<2> const &dom, float)
+  {
+    int const axis = A == vsip::col ? 0 : 1;
+    return fcb_supported_real_length((long long)dom[axis].size()) && dom[1 - axis].size() > 0;
+  }
+  static std::unique_ptr<backend_type> exec(Domain<2> const &dom, float scale)
+  {
+    return std::unique_ptr<backend_type>(new fcb200::fftm_c2r<A>(dom, scale));
   }
 };
 

@@ -45,12 +45,14 @@ def _is_torch(x) -> bool:
     return type(x).__module__.startswith("torch")
 
 
-def _desc(x, writable: bool):
-    """(pointer, rows, cols, row_stride, where) of a 2-D complex64 array/tensor."""
+def _desc(x, writable: bool, real: bool = False):
+    """(pointer, rows, cols, row_stride, where) of a 2-D complex64 (or, with
+    real=True, float32) array/tensor; the stride counts elements."""
+    el = 4 if real else 8
     if _is_torch(x):
         import torch
-        if x.dtype != torch.complex64:
-            raise TypeError("expected a complex64 tensor")
+        if x.dtype != (torch.float32 if real else torch.complex64):
+            raise TypeError("expected a float32 tensor" if real else "expected a complex64 tensor")
         if not x.is_cuda:
             raise TypeError("torch tensors must be on a CUDA device; use numpy arrays for host data")
         if x.dim() == 1:
@@ -60,15 +62,15 @@ def _desc(x, writable: bool):
         rs = x.stride(0) if x.shape[0] > 1 else x.shape[1]
         return x.data_ptr(), x.shape[0], x.shape[1], rs, _lib.FCB_DEVICE
     a = x
-    if not isinstance(a, np.ndarray) or a.dtype != np.complex64:
-        raise TypeError("expected a numpy complex64 array")
+    if not isinstance(a, np.ndarray) or a.dtype != (np.float32 if real else np.complex64):
+        raise TypeError("expected a numpy float32 array" if real else "expected a numpy complex64 array")
     if a.ndim == 1:
         a = a.reshape(1, -1)
-    if a.ndim != 2 or (a.shape[1] > 1 and a.strides[1] != 8) or a.strides[0] % 8:
+    if a.ndim != 2 or (a.shape[1] > 1 and a.strides[1] != el) or a.strides[0] % el:
         raise ValueError("expected a 2-D array with unit-stride rows")
     if writable and not a.flags.writeable:
         raise ValueError("output array is read-only")
-    rs = a.strides[0] // 8 if a.shape[0] > 1 else a.shape[1]  # one row: any stride is fine
+    rs = a.strides[0] // el if a.shape[0] > 1 else a.shape[1]  # one row: any stride is fine
     return a.ctypes.data, a.shape[0], a.shape[1], rs, _lib.FCB_HOST
 
 
@@ -83,6 +85,30 @@ def _empty_like(x):
         import torch
         return torch.empty_like(x, memory_format=torch.contiguous_format)
     return np.empty(x.shape, dtype=np.complex64)
+
+
+def _empty(like, shape, real: bool):
+    """New array (numpy) or CUDA tensor on like's device, float32 or complex64."""
+    if _is_torch(like):
+        import torch
+        return torch.empty(shape, dtype=torch.float32 if real else torch.complex64, device=like.device)
+    return np.empty(shape, dtype=np.float32 if real else np.complex64)
+
+
+def _transposed(x):
+    """Contiguous transpose: the column-major copy the reference's DDA layer makes
+    for a column-axis Fftm (query_layout asks for tuple<1,0,2>)."""
+    if _is_torch(x):
+        return x.t().contiguous()
+    return np.ascontiguousarray(x.T)
+
+
+def _put_transposed(out, yt):
+    if _is_torch(out):
+        out.copy_(yt.t())
+    else:
+        out[...] = yt.T
+    return out
 
 
 class _Plan:
@@ -112,8 +138,9 @@ class _Plan:
         op, r2, c2, ors, ow = _desc(out, True)
         if (r, c) != (r2, c2):
             raise ValueError(f"shape mismatch {(r, c)} vs {(r2, c2)}")
-        if c != self.cols:
-            raise ValueError(f"row length {c} != planned {self.cols}")
+        n = getattr(self, "_n", self.cols)  # transform length (Fftm along columns: rows)
+        if c != n:
+            raise ValueError(f"row length {c} != planned {n}")
         if iw != ow:
             raise ValueError("input and output must both be host arrays or both device tensors")
         _bind_stream(self._handle, iw)
@@ -125,26 +152,101 @@ class _Plan:
         raise NotImplementedError
 
 
-class Fftm(_Plan):
-    """Row-wise multiple FFT on the GPU (vsip::Fftm<C, C, row, D, R>)."""
+row = 0  # axis tags, values of vsip::row / vsip::col (src/vsip/support.hpp:167-168):
+col = 1  # Fftm<I, O, row, ...> transforms each row, Fftm<I, O, col, ...> each column
 
-    def __init__(self, rows: int, cols: int, direction: int = fft_fwd, scale: float = 1.0):
+
+class Fftm(_Plan):
+    """Multiple FFT on the GPU (vsip::Fftm<C, C, A, D, R>).
+
+    axis=row (default) transforms each of the `rows` rows of length `cols`;
+    axis=col transforms each of the `cols` columns of length `rows`.  Column
+    data is transposed into contiguous rows and back around the row kernel, as
+    the reference's DDA layer does for its FFTW backend."""
+
+    def __init__(self, rows: int, cols: int, direction: int = fft_fwd, scale: float = 1.0, axis: int = row):
         self.rows, self.cols = int(rows), int(cols)
+        self.axis = _axis(axis)
         self.exponent = _exponent(direction)
         self.scale = float(scale)
+        n, count = (self.cols, self.rows) if self.axis == row else (self.rows, self.cols)
         h = ctypes.c_void_p()
-        check(lib().fcb_plan_fftm(self.cols, self.rows, self.exponent, self.scale, ctypes.byref(h)))
+        check(lib().fcb_plan_fftm(n, count, self.exponent, self.scale, ctypes.byref(h)))
         self._handle = h
+        self._n = n
 
     def __call__(self, inp, out=None):
-        """By reference: ``fftm(in, out)``.  ``fftm(inout, inplace=True)`` is the
-        in-place form; ``fftm(in)`` returns a new result (by value)."""
+        """By reference: ``fftm(in, out)``; ``fftm(in)`` returns a new result (by value)."""
         if out is None:
             out = _empty_like(inp)
+        if self.axis == col:
+            return _put_transposed(out, self._rows(_transposed(inp)))
         return self._exec(inp, out)
 
     def in_place(self, inout):
+        if self.axis == col:
+            return _put_transposed(inout, self._rows(_transposed(inout)))
         return self._exec(inout, inout)
+
+    def _rows(self, xt):
+        return self._exec(xt, _empty_like(xt))
+
+
+def _axis(axis: int) -> int:
+    if axis not in (row, col):
+        raise ValueError("axis must be row (0) or col (1)")
+    return axis
+
+
+class FftmReal(_Plan):
+    """Real-input multiple FFT on the GPU.
+
+    direction fft_fwd: vsip::Fftm<float, complex<float>, A, fft_fwd> -- real
+    input of `rows` x `cols`, complex output with n/2 + 1 bins along the axis.
+    direction fft_inv: vsip::Fftm<complex<float>, float, A, fft_inv> -- the
+    half spectrum in, real output of `rows` x `cols` (unnormalised; pass
+    scale=1/n for the inverse of the forward).  rows x cols is always the real
+    side's domain, as in the reference; axis as for Fftm."""
+
+    def __init__(self, rows: int, cols: int, direction: int = fft_fwd, scale: float = 1.0, axis: int = row):
+        self.rows, self.cols = int(rows), int(cols)
+        self.axis = _axis(axis)
+        self.exponent = _exponent(direction)
+        self.scale = float(scale)
+        self.n, self.count = (self.cols, self.rows) if self.axis == row else (self.rows, self.cols)
+        self.bins = self.n // 2 + 1
+        h = ctypes.c_void_p()
+        check(lib().fcb_plan_fftm_real(self.n, self.count, self.exponent, self.scale, ctypes.byref(h)))
+        self._handle = h
+
+    def output_shape(self):
+        if self.exponent == _lib.FCB_INVERSE:
+            return (self.rows, self.cols)
+        return (self.count, self.bins) if self.axis == row else (self.bins, self.count)
+
+    def __call__(self, inp, out=None):
+        fwd = self.exponent == _lib.FCB_FORWARD
+        if out is None:
+            out = _empty(inp, self.output_shape(), real=not fwd)
+        if self.axis == col:
+            yt = _empty(inp, (self.count, self.n if not fwd else self.bins), real=not fwd)
+            self._rows(_transposed(inp), yt)
+            return _put_transposed(out, yt)
+        return self._rows(inp, out)
+
+    def _rows(self, inp, out):
+        fwd = self.exponent == _lib.FCB_FORWARD
+        ip, r, c, irs, iw = _desc(inp, False, real=fwd)
+        op, r2, c2, ors, ow = _desc(out, True, real=not fwd)
+        want_in, want_out = (self.n, self.bins) if fwd else (self.bins, self.n)
+        if c != want_in or c2 != want_out or r != r2:
+            raise ValueError(f"shapes {(r, c)} -> {(r2, c2)} do not match n={self.n}")
+        if iw != ow:
+            raise ValueError("input and output must both be host arrays or both device tensors")
+        _bind_stream(self._handle, iw)
+        fn = lib().fcb_exec_r2c if fwd else lib().fcb_exec_c2r
+        check(fn(self._handle, ctypes.c_void_p(ip), irs, ctypes.c_void_p(op), ors, r, iw))
+        return out
 
 
 class Fft2d(_Plan):
@@ -237,5 +339,6 @@ def supported_length(n: int) -> bool:
     return bool(lib().fcb_supported_length(int(n)))
 
 
-__all__ = ["Fftm", "Fft2d", "Fastconv", "vmmul", "replica_spectrum", "supported_length", "fft_fwd", "fft_inv",
+__all__ = ["Fftm", "FftmReal", "Fft2d", "Fastconv", "vmmul", "replica_spectrum", "supported_length", "fft_fwd",
+           "fft_inv", "row", "col",
            "FcbError"]

@@ -48,9 +48,26 @@ def test_reference_fastconv_test_on_b200():
 
 @pytest.mark.gpu
 def test_reference_fftm_test_on_b200():
+    # rows and columns, powers of two and not (18, 68, 252: Bluestein), and
+    # test_real's real <-> complex Fftm along columns (16, 128, 242)
     r = _run([_prog("fftm_test")])
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "[fcb200] Fftm<fwd>" in r.stderr and "[fcb200] Fftm<inv>" in r.stderr
+    assert "[fcb200] Fftm<fwd, col> 68 x" in r.stderr and "[fcb200] Fftm<inv, col>" in r.stderr
+    assert "Fftm<fwd> 5 x 252" in r.stderr or "x 252 scale" in r.stderr
+    for n in (16, 128, 242):
+        assert f"[fcb200] Fftm<real->complex, col> n {n} x 5" in r.stderr
+        assert f"[fcb200] Fftm<complex->real, col> n {n} x 5" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["fftm_unaligned", "fft_ip_subview", "fft_temp_view"])
+def test_reference_fftm_regressions_on_b200(name):
+    # tests/regressions: unaligned and gapped rows in interleaved and split
+    # storage, in-place subviews, temporary views (rows and columns)
+    r = _run([_prog("reg_" + name)])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "[fcb200] Fftm<" in r.stderr
 
 
 @pytest.mark.gpu
