@@ -448,6 +448,8 @@ def main():
     ap.add_argument("--serve", action="store_true", help="served-stream line instead of the benchmark")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--pulses", type=int, default=PULSES, help="override the pulse count (profiling other shapes)")
+    ap.add_argument("--samples", type=int, default=NSAMP, help="override the samples per pulse")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -476,12 +478,14 @@ def main():
     import openvsip_b200 as ov
     from openvsip_b200 import synth
 
+    pulses, nsamp = args.pulses, args.samples
+    default_shape = (pulses, nsamp) == (PULSES, NSAMP)
     if args.threads:
-        ov.lib().fcb_tune_set(NSAMP, 2, args.threads)
-    job = synth.large_fastconv(seed=1000 + rank, pulses=PULSES, n=NSAMP, tbp=TBP, echoes=ECHOES)
+        ov.lib().fcb_tune_set(nsamp, 2, args.threads)
+    job = synth.large_fastconv(seed=1000 + rank, pulses=pulses, n=nsamp, tbp=TBP, echoes=ECHOES)
     x_host = job["data"]
     rep = job["replica_spectrum"]
-    fc = ov.Fastconv(rep, PULSES)
+    fc = ov.Fastconv(rep, pulses)
     info = fc.info()
     xin = [torch.from_numpy(x_host).cuda(), torch.from_numpy(np.roll(x_host, 1, axis=0)).cuda()]
     yout = torch.empty_like(xin[0])
@@ -525,10 +529,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t.item())
 
-    samples_step = PULSES * NSAMP
+    samples_step = pulses * nsamp
     value = samples_step * args.steps * world / (total_ms / 1e3)
     launch_ms = sum(step_ms) / len(step_ms)
-    alg_bytes = 16.0 * samples_step + 8.0 * NSAMP
+    alg_bytes = 16.0 * samples_step + 8.0 * nsamp
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     peak, peak_src = measured_peak()
 
@@ -560,16 +564,20 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
             "data": "synthetic (seeded complex Gaussian + LFM echoes)",
-            "config": {"workload": WORKLOAD, "pulses": PULSES, "samples": NSAMP, "tbp": TBP,
+            "config": {"workload": WORKLOAD if default_shape else WORKLOAD.replace(
+                           f"{PULSES} pulses x {NSAMP} samples", f"{pulses} pulses x {nsamp} samples"),
+                       "pulses": pulses, "samples": nsamp, "tbp": TBP,
                        "parallelism": f"{world} independent batches (weak)",
-                       "l2": "inputs larger than L2 (256 MB read+write per step, 2 alternating inputs)",
+                       "l2": f"inputs larger than L2 ({16 * samples_step >> 20} MB read+write per step, "
+                             "2 alternating inputs)",
                        "kernel": {"threads": info["threads"], "cluster_ctas": info["cluster_ctas"],
                                   "smem_bytes": info["smem_bytes"]}},
             "latency_ms": {"p50": sorted_ms[len(sorted_ms) // 2],
                            "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))]},
             "rel_l2_vs_fp64": rel,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": ncu_traffic(), "peak_source": peak_src,
+                         "frac": achieved / peak, "traffic": ncu_traffic() if default_shape else None,
+                         "peak_source": peak_src,
                          "alg_bytes_per_launch": alg_bytes, "launch_ms": launch_ms},
             "cpu_baseline": cpu,
             "fftw_standin": standin,

@@ -13,6 +13,10 @@ the reference tree; the fixtures themselves are committed and travel).
      the 64 x 2048 CPU configuration,
      the shift-kernel fused fast convolution 16 x 64 (tests/fastconv.cpp:341-366),
      the matrix-of-coefficients form 16 x 64 (tests/fastconv.cpp:213-246).
+3. matched_filter_ref.txt -- the printed output of the reference's radar
+   matched-filter example (share/examples/radar/matched_filter.cpp, 100
+   Doppler rows x 1000 samples), built by oracle/Makefile on the reference's
+   generic backend (oracle/_ref/matched_filter).
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -113,9 +117,17 @@ def ref_outputs():
     np.savez_compressed(os.path.join(HERE, "ref_outputs.npz"), **out)
 
 
+def matched_filter():
+    prog = os.path.join(ROOT, "oracle", "_ref", "matched_filter")
+    out = subprocess.run([prog], capture_output=True, text=True, check=True).stdout
+    with open(os.path.join(HERE, "matched_filter_ref.txt"), "w") as f:
+        f.write(out)
+
+
 if __name__ == "__main__":
     fft_ext()
-    if not os.path.exists(DRIVER):
+    if not os.path.exists(DRIVER) or not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "matched_filter")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}"], check=True)
     ref_outputs()
+    matched_filter()
     print("fixtures written to", HERE)

@@ -61,6 +61,19 @@ def test_reference_fftm_test_on_b200():
 
 
 @pytest.mark.gpu
+def test_reference_matched_filter_example_on_b200():
+    # share/examples/radar/matched_filter.cpp: a matched-filter bank over 100
+    # Doppler shifts x 1000 delays (coefficients by a forward Fftm, output by
+    # an inverse Fftm of vmmul<0>); its printed delays must equal those of the
+    # same program on the reference's own backend (tests/golden/matched_filter_ref.txt)
+    r = _run([_prog("ex_matched_filter")])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    want = open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "matched_filter_ref.txt")).read()
+    assert r.stdout == want
+    assert "[fcb200] Fftm<fwd> 100 x 1000" in r.stderr and "[fcb200] Fftm<inv> 100 x 1000" in r.stderr
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", ["fftm_unaligned", "fft_ip_subview", "fft_temp_view"])
 def test_reference_fftm_regressions_on_b200(name):
     # tests/regressions: unaligned and gapped rows in interleaved and split
