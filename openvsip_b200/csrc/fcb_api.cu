@@ -444,7 +444,7 @@ int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long
   a.rep_rs = rep_rs;
   a.scale = p->scale;
   a.vec_out = (reinterpret_cast<uintptr_t>(out) % 16 == 0) && (out_rs % 2 == 0 || rows == 1);
-  a.ahead = -1;  // launch_rows picks one resident wave
+  a.ahead = -1;  // launch_rows picks half a resident wave
   return launch_rows(p->k, rows, a, st);
 }
 

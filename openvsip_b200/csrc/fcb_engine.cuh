@@ -320,8 +320,8 @@ struct RowArgs
   int transpose_out;    // standalone FFT: store the result transposed (2-D FFT passes)
   int vec_out;          // standalone FFT: every output row starts 16-byte aligned
   long long ahead;      // L2 prefetch distance in tiles (CTAs, or clusters) -- about
-                        // one resident wave, so that tile's rows stream from HBM
-                        // into L2 while this tile computes; 0 = off
+                        // half a resident wave, so that tile's rows stream from
+                        // HBM into L2 while this tile computes; 0 = off
 };
 
 __device__ __forceinline__ void prefetch_l2(const void *p)
@@ -419,21 +419,6 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     asm volatile("cp.async.commit_group;" ::: "memory");
   }
 
-  // prefetch into L2 the input of the tile that runs about one wave later
-  if (a.ahead > 0)
-  {
-    const long long row0 = (tile + a.ahead) * S::ROWS;
-    constexpr int LPR = S::N >= 16 ? S::N / 16 : 1;          // 128-byte lines per row
-    constexpr int LINES = S::ROWS * LPR / S::CS;             // lines of this CTA's part
-#pragma unroll 1
-    for (int i = t; i < LINES; i += THREADS)
-    {
-      const int li = rank * LINES + i;
-      const long long r = row0 + li / LPR;
-      if (r < a.rows) prefetch_l2(a.in + r * a.in_rs + (long long)(li % LPR) * 16);
-    }
-  }
-
   cpair c[S::CPT];
 
   // ---------------- stage 1 (direction SIGN) ----------------
@@ -443,6 +428,24 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 #pragma unroll
     for (int j = 0; j < S::EPT; ++j)
       x[j] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
+    // With this tile's loads in flight, prefetch into L2 the input of the tile
+    // `ahead` tiles later (about half a resident wave), so that it streams in
+    // from HBM while this tile computes.  Straight-line code (a few lines per
+    // thread) placed here measured faster than a loop at the kernel start.
+    {
+      constexpr int LPR = S::N >= 16 ? S::N / 16 : 1;          // 128-byte lines per row
+      constexpr int LINES = S::ROWS * LPR / S::CS;             // lines of this CTA's part
+      constexpr int PER = (LINES + THREADS - 1) / THREADS;
+      const long long row0 = (tile + a.ahead) * S::ROWS;
+#pragma unroll
+      for (int k = 0; k < PER; ++k)
+      {
+        const int i = t + THREADS * k;
+        const int li = rank * LINES + i;
+        const long long r = row0 + li / LPR;
+        if (a.ahead > 0 && i < LINES && r < a.rows) prefetch_l2(a.in + r * a.in_rs + (li % LPR) * 16);
+      }
+    }
     // W_N^{tr q} for q = 2q' + lane; groups g > 0 add the constant W_32^{g q}
     float4 tw1[S::H1];
     if constexpr (S::NS > 1)
