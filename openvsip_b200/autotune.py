@@ -3,10 +3,12 @@
 What it chooses (measured on the device with CUDA events, never guessed):
 
 * For each row length and kind (forward Fftm, inverse Fftm, fused fastconv),
-  the tile schedule of the row kernel: CTAs of 256 threads (8192 samples per
-  CTA, two CTAs per SM; rows longer than that split over a thread-block
-  cluster) or of 512 threads (16384 samples per CTA, one CTA per SM).  The
-  choice is installed with fcb_tune_set and applies to plans made afterwards.
+  the tile schedule of the row kernel: CTAs of 128 threads (4096 samples per
+  CTA, four CTAs per SM; rows of 256 .. 16384 samples), 256 threads (8192
+  samples, two per SM) or 512 threads (16384 samples, one per SM; rows of 4096
+  samples and more).  Rows longer than one CTA's samples split over a
+  thread-block cluster.  The choice is installed with fcb_tune_set and applies
+  to plans made afterwards.
 * For the batched launch: the same CTA size (which also fixes the cluster
   shape: 4 x 256 or 2 x 512 threads for 32768-sample rows) and the job order
   (longest rows first, or as given).
@@ -24,7 +26,17 @@ from . import _lib
 from ._lib import lib
 
 KINDS = {"forward": 0, "inverse": 1, "fastconv": 2}
-VARIANT_MIN_N = 4096  # 512-thread variants exist from 4096 samples up
+VARIANT_MIN_N = 256  # below this every length has only the 256-thread kernel
+
+
+def variants(n: int) -> tuple:
+    """CTA sizes the library has kernels for at row length n."""
+    out = [256]
+    if 256 <= n <= 16384:
+        out.insert(0, 128)
+    if n >= 4096:
+        out.append(512)
+    return tuple(out)
 
 
 def cache_path() -> str:
@@ -67,14 +79,14 @@ def time_plan(kind: str, n: int, threads: int, samples: int = 1 << 24, reps: int
     return _time_ms(lambda: plan(x, y), reps)
 
 
-def tune_plans(lengths=(8192, 16384, 32768, 65536), kinds=tuple(KINDS), samples: int = 1 << 24) -> dict:
+def tune_plans(lengths=(1024, 4096, 8192, 16384, 32768, 65536), kinds=tuple(KINDS), samples: int = 1 << 24) -> dict:
     """Pick the CTA size per (kind, length); installs and returns the choices."""
     out = {}
     for kind in kinds:
         for n in lengths:
             if n < VARIANT_MIN_N:
                 continue
-            times = {t: time_plan(kind, n, t, samples) for t in (256, 512)}
+            times = {t: time_plan(kind, n, t, samples) for t in variants(n)}
             best = min(times, key=times.get)
             _lib.check(lib().fcb_tune_set(n, KINDS[kind], best))
             out[f"{kind}:{n}"] = {"threads": best, "ms": times}

@@ -271,9 +271,10 @@ static void init_table()
     for (int l = 0; l <= kMaxLogN; ++l)
       for (int m = 0; m < 3; ++m)
         // defaults (measured): 4 CTAs of 128 threads per SM for rows of 256 ..
-        // 4096 samples, one 512-thread CTA per 16384-sample row, else 256
-        // (128-thread clusters for 8192 and 16384 samples measured slower)
-        g_variant[l][m] = (l == 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
+        // 4096 samples, 256-thread CTAs for 8192, 512-thread CTAs from 16384
+        // up (clusters of 2 and 4 of them for 32768 and 65536; clusters of
+        // smaller CTAs measured slower at every length)
+        g_variant[l][m] = (l >= 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
   });
 }
 
