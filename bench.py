@@ -476,7 +476,7 @@ def main():
                                 device_id=torch.device("cuda", local))
 
     import openvsip_b200 as ov
-    from openvsip_b200 import synth
+    from openvsip_b200 import shard, synth
 
     pulses, nsamp = args.pulses, args.samples
     default_shape = (pulses, nsamp) == (PULSES, NSAMP)
@@ -524,10 +524,7 @@ def main():
     barrier()
     total_ms = t_start.elapsed_time(t_end)
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    t = torch.tensor([total_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = shard.max_over_ranks(total_ms)  # max over ranks (NCCL all-reduce of one scalar)
 
     samples_step = pulses * nsamp
     value = samples_step * args.steps * world / (total_ms / 1e3)
@@ -546,10 +543,7 @@ def main():
     for _ in range(e2e_steps):
         fc(hin, hout)
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = samples_step * e2e_steps * world / float(te.item())
+    e2e_value = samples_step * e2e_steps * world / shard.max_over_ranks(e2e_s)
 
     if rank == 0:
         cpu = None
