@@ -7,7 +7,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <new>
+#include <vector>
 
 using namespace fcb;
 
@@ -25,10 +27,14 @@ struct fcb_plan_s
   long long rep_rows = 0;         // 1 = shared vector, else one per data row
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;  // current stream (own or caller's)
-  cudaStream_t aux = nullptr;     // second stream for host pipelining
-  float2 *stage[2] = {nullptr, nullptr};
+  // host calls: chunks pipelined through kMaxStage device buffers, copies in
+  // on cin, kernels on the plan stream, copies out on cout
+  static constexpr int kMaxStage = 4;
+  cudaStream_t cin = nullptr, cout = nullptr;
+  float2 *stage[kMaxStage] = {};
   long long stage_rows = 0;
-  cudaEvent_t done[2] = {nullptr, nullptr};
+  int nstage = 0;
+  cudaEvent_t ev_in[kMaxStage] = {}, ev_k[kMaxStage] = {}, ev_out[kMaxStage] = {}, ev_start = nullptr;
   // 2-D FFT (rows x cols): pass 1 transforms rows into a transposed scratch
   // matrix, pass 2 transforms its rows (the columns) back transposed.
   bool is2d = false;
@@ -112,15 +118,15 @@ void plan_free(fcb_plan p)
   if (!p) return;
   DeviceGuard g(p->device);
   if (p->own_stream) cudaStreamSynchronize(p->own_stream);
-  if (p->aux) cudaStreamSynchronize(p->aux);
+  if (p->cin) cudaStreamSynchronize(p->cin);
+  if (p->cout) cudaStreamSynchronize(p->cout);
   cudaFree(p->tw);
   cudaFree(p->twc);
   cudaFree(p->scratch);
   cudaFree(p->stage2d_in);
   cudaFree(p->stage2d_out);
   cudaFree(p->rep);
-  cudaFree(p->stage[0]);
-  cudaFree(p->stage[1]);
+  for (auto b : p->stage) cudaFree(b);
   for (int d = 0; d < 2; ++d)
   {
     plan_free(p->inner[d]);
@@ -133,9 +139,16 @@ void plan_free(fcb_plan p)
   cudaFree(p->rbuf);
   cudaFree(p->rstage[0]);
   cudaFree(p->rstage[1]);
-  for (auto &e : p->done) if (e) cudaEventDestroy(e);
+  for (int i = 0; i < fcb_plan_s::kMaxStage; ++i)
+  {
+    if (p->ev_in[i]) cudaEventDestroy(p->ev_in[i]);
+    if (p->ev_k[i]) cudaEventDestroy(p->ev_k[i]);
+    if (p->ev_out[i]) cudaEventDestroy(p->ev_out[i]);
+  }
+  if (p->ev_start) cudaEventDestroy(p->ev_start);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
-  if (p->aux) cudaStreamDestroy(p->aux);
+  if (p->cin) cudaStreamDestroy(p->cin);
+  if (p->cout) cudaStreamDestroy(p->cout);
   delete p;
 }
 
@@ -448,68 +461,131 @@ int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long
   return launch_rows(p->k, rows, a, st);
 }
 
-int ensure_staging(fcb_plan p, long long chunk_rows)
+// Host staging shape: chunk bytes and pipeline depth.  FCB200_STAGE_MB and
+// FCB200_STAGES override the defaults (16 MB, 3 buffers).
+long long stage_bytes()
 {
-  if (p->stage_rows >= chunk_rows) return FCB_OK;
-  cudaFree(p->stage[0]);
-  cudaFree(p->stage[1]);
-  p->stage[0] = p->stage[1] = nullptr;
+  static const long long v = [] {
+    const char *e = std::getenv("FCB200_STAGE_MB");
+    const long long mb = e ? std::atoll(e) : 16;
+    return std::max<long long>(1, mb) << 20;
+  }();
+  return v;
+}
+int stage_depth()
+{
+  static const int v = [] {
+    const char *e = std::getenv("FCB200_STAGES");
+    const int d = e ? std::atoi(e) : 3;
+    return std::min(std::max(d, 2), (int)fcb_plan_s::kMaxStage);
+  }();
+  return v;
+}
+
+int ensure_staging(fcb_plan p, long long chunk_rows, int depth)
+{
+  if (p->stage_rows >= chunk_rows && p->nstage >= depth) return FCB_OK;
+  for (auto &b : p->stage)
+  {
+    cudaFree(b);
+    b = nullptr;
+  }
   p->stage_rows = 0;
-  for (int i = 0; i < 2; ++i)
+  p->nstage = 0;
+  for (int i = 0; i < depth; ++i)
   {
     cudaError_t e = cudaMalloc(&p->stage[i], sizeof(float2) * (size_t)(chunk_rows * p->n));
     if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "staging buffer: %s", cudaGetErrorString(e));
   }
-  if (!p->aux)
+  if (!p->cin)
   {
-    cudaError_t e = cudaStreamCreateWithFlags(&p->aux, cudaStreamNonBlocking);
-    if (e != cudaSuccess) return cuda_error(e, "cudaStreamCreate");
-    for (auto &ev : p->done)
-      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
-        return cuda_error(e, "cudaEventCreate");
-  }
-  if (p->blue_m && !p->blue_buf[1])
-  {
-    cudaError_t e = cudaMalloc(&p->blue_buf[1], sizeof(float2) * (size_t)(p->blue_chunk * p->blue_m));
-    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "Bluestein work rows: %s", cudaGetErrorString(e));
+    cudaError_t e = cudaStreamCreateWithFlags(&p->cin, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cout, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_start, cudaEventDisableTiming);
+    for (int i = 0; e == cudaSuccess && i < fcb_plan_s::kMaxStage; ++i)
+    {
+      e = cudaEventCreateWithFlags(&p->ev_in[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_k[i], cudaEventDisableTiming);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->ev_out[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return cuda_error(e, "staging streams");
   }
   p->stage_rows = chunk_rows;
+  p->nstage = depth;
   return FCB_OK;
 }
 
-// Host-pointer execution: rows move through two device staging buffers in
-// chunks on two streams, so one chunk's copies overlap the other's kernel.
+// Host-pointer execution: rows move through `depth` device buffers in chunks.
+// Copies in run on cin, kernels on the plan stream, copies out on cout, linked
+// by events, so both copy directions and the kernels overlap and the PCIe link
+// stays busy in both directions; a buffer is refilled once its copy out is done.
 int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
               long long rows)
 {
   const size_t row_bytes = sizeof(float2) * (size_t)p->n;
-  long long chunk = std::max<long long>(1, (16LL << 20) / (long long)row_bytes);
+  long long chunk = std::max<long long>(1, stage_bytes() / (long long)row_bytes);
   if (p->k && p->k->cluster == 1) chunk = std::max<long long>(chunk, p->k->rows_per_cta);
   chunk = std::min(chunk, rows);
-  int rc = ensure_staging(p, chunk);
+  const int depth = stage_depth();
+  int rc = ensure_staging(p, chunk, depth);
   if (rc) return rc;
-  cudaStream_t st[2] = {p->stream, p->aux};
-  // the aux stream must not start before earlier work on the plan stream
-  cudaEventRecord(p->done[1], p->stream);
-  cudaStreamWaitEvent(p->aux, p->done[1], 0);
-  int i = 0;
-  for (long long r0 = 0; r0 < rows; r0 += chunk, i ^= 1)
+  // nothing starts before earlier work on the plan stream
+  cudaEventRecord(p->ev_start, p->stream);
+  cudaStreamWaitEvent(p->cin, p->ev_start, 0);
+  cudaStreamWaitEvent(p->cout, p->ev_start, 0);
+  // Chunk sizes ramp up over the first chunks and down over the last ones
+  // (1/8, 1/4, 1/2 of a full chunk), so the first copy out and the last copy
+  // in overlap the other direction sooner: the link idles in one direction
+  // only for a small chunk at each end of the call.
+  const long long unit = std::max<long long>(1, (p->k && p->k->cluster == 1) ? p->k->rows_per_cta : 1);
+  std::vector<long long> sizes;
   {
-    long long nr = std::min(chunk, rows - r0);
-    float2 *buf = p->stage[i];
-    cudaError_t e = cudaMemcpy2DAsync(buf, row_bytes, in + r0 * in_rs, sizeof(float2) * (size_t)in_rs,
-                                      row_bytes, (size_t)nr, cudaMemcpyHostToDevice, st[i]);
-    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
-    rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, st[i], i);
-    if (rc) return rc;
-    e = cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,
-                          (size_t)nr, cudaMemcpyDeviceToHost, st[i]);
-    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    const long long ramp[3] = {chunk / 8, chunk / 4, chunk / 2};
+    long long head = 0;
+    for (long long v : ramp) head += std::max(unit, v);
+    if (rows >= 2 * head + chunk)
+    {
+      long long left = rows;
+      for (long long v : ramp) { sizes.push_back(std::max(unit, v)); left -= sizes.back(); }
+      left -= head;  // reserved for the tail ramp
+      while (left > 0) { sizes.push_back(std::min(chunk, left)); left -= sizes.back(); }
+      for (int i = 2; i >= 0; --i) sizes.push_back(std::max(unit, ramp[i]));
+    }
+    else
+      for (long long left = rows; left > 0; left -= sizes.back()) sizes.push_back(std::min(chunk, left));
   }
-  cudaError_t e1 = cudaStreamSynchronize(st[0]);
-  cudaError_t e2 = cudaStreamSynchronize(st[1]);
+  long long r0 = 0;
+  for (size_t c = 0; c < sizes.size(); r0 += sizes[c], ++c)
+  {
+    const int b = (int)(c % depth);
+    const long long nr = sizes[c];
+    float2 *buf = p->stage[b];
+    if ((int)c >= depth) cudaStreamWaitEvent(p->cin, p->ev_out[b], 0);  // buffer drained
+    // dense rows move as one linear copy, strided rows as a pitched one
+    cudaError_t e = in_rs == p->n
+                      ? cudaMemcpyAsync(buf, in + r0 * in_rs, row_bytes * (size_t)nr, cudaMemcpyHostToDevice, p->cin)
+                      : cudaMemcpy2DAsync(buf, row_bytes, in + r0 * in_rs, sizeof(float2) * (size_t)in_rs, row_bytes,
+                                          (size_t)nr, cudaMemcpyHostToDevice, p->cin);
+    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    cudaEventRecord(p->ev_in[b], p->cin);
+    cudaStreamWaitEvent(p->stream, p->ev_in[b], 0);
+    rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, p->stream, 0);
+    if (rc) return rc;
+    cudaEventRecord(p->ev_k[b], p->stream);
+    cudaStreamWaitEvent(p->cout, p->ev_k[b], 0);
+    e = out_rs == p->n
+          ? cudaMemcpyAsync(out + r0 * out_rs, buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
+          : cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,
+                              (size_t)nr, cudaMemcpyDeviceToHost, p->cout);
+    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    cudaEventRecord(p->ev_out[b], p->cout);
+  }
+  cudaError_t e1 = cudaStreamSynchronize(p->cout);
+  cudaError_t e2 = cudaStreamSynchronize(p->stream);
+  cudaError_t e3 = cudaStreamSynchronize(p->cin);
   if (e1 != cudaSuccess) return cuda_error(e1, "fcb_exec (host)");
   if (e2 != cudaSuccess) return cuda_error(e2, "fcb_exec (host)");
+  if (e3 != cudaSuccess) return cuda_error(e3, "fcb_exec (host)");
   return FCB_OK;
 }
 
