@@ -387,7 +387,9 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     a.rep = b->replicas[j.replica].table;
     a.rep_rs = 0;
     a.scale = 1.f;
-    a.ahead = 0;
+    // L2 prefetch of the same job's rows about half a wave of units later
+    // (units are taken in order; across a job boundary nothing is prefetched)
+    a.ahead = (long long)std::max(1, b->grid / b->v.csmax / 2) * bj.tiles_per_unit;
     hj.push_back(bj);
   }
   cudaSetDevice(b->device);
