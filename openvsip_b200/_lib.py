@@ -1,8 +1,7 @@
 """ctypes binding of libfcb200.so (the C ABI declared in include/fcb200.h).
 
-The library must have been built (``python -m openvsip_b200.build`` or
-``__graft_entry__.build()``); loading fails loudly otherwise.  There is no CPU
-fallback anywhere in this package.
+The library must have been built (``python -m openvsip_b200.build``); loading
+fails loudly otherwise.  There is no CPU fallback anywhere in this package.
 """
 from __future__ import annotations
 
