@@ -231,8 +231,6 @@ static KernelInfo make_info()
   return k;
 }
 
-constexpr int kMin512 = 12;  // 512-thread variants exist for rows of 4096 samples and more
-constexpr int kMin128 = 8, kMax128 = 14;  // 128-thread variants: rows of 256 .. 16384 samples
 
 template <int LOGN>
 static void fill_table(KernelInfo (*tab)[3][3])

@@ -43,15 +43,18 @@ struct fcb_plan_s
   float4 *twc = nullptr;
   float2 *scratch = nullptr;
   float2 *stage2d_in = nullptr, *stage2d_out = nullptr;
-  // Rows of non-power-of-two length n (Bluestein): chirp pre-multiply into
-  // work rows of blue_m >= 2n - 1 samples, fused length-blue_m pass(es),
-  // chirp post-multiply.  Index 0 is the forward direction, 1 the inverse.
+  // Rows of non-power-of-two length n (Bluestein): the fused kernel's
+  // kChirpconv mode runs on work rows of blue_m >= 2n - 1 samples, reading the
+  // n samples times a chirp (zero beyond) and writing n samples times a chirp.
+  // Index 0 is the forward direction, 1 the inverse.
   long long blue_m = 0;
-  long long blue_chunk = 0;                    // rows per work-buffer pass
+  long long blue_chunk = 0;                    // fastconv: rows per pass through blue_buf
   float2 *chirp[2] = {nullptr, nullptr};       // c[k] = e^{-+ i pi k^2 / n}
-  fcb_plan inner[2] = {nullptr, nullptr};      // length-blue_m fastconv, replica FFT(conj(c))
+  float2 *chirp_out = nullptr;                 // Fftm: c[k] * scale (the output multiplier)
+  fcb_plan inner[2] = {nullptr, nullptr};      // length-blue_m tables: twiddles, replica FFT(conj(c))
+  const KernelInfo *kchirp = nullptr;          // the kChirpconv kernel for blue_m
   float2 *blue_rep = nullptr;                  // fastconv: replica spectra / n, rows of n
-  float2 *blue_buf[2] = {nullptr, nullptr};    // work rows, one per staging stream
+  float2 *blue_buf[2] = {nullptr, nullptr};    // fastconv: rows of n between its two passes
   // Real-input rows of n = rn samples: 1 = real -> complex (n/2 + 1 outputs),
   // 2 = complex -> real.  Even n: a length-n/2 complex plan plus the split /
   // merge step; odd n: a length-n complex plan on expanded rows.
@@ -134,6 +137,7 @@ void plan_free(fcb_plan p)
     cudaFree(p->blue_buf[d]);
   }
   cudaFree(p->blue_rep);
+  cudaFree(p->chirp_out);
   plan_free(p->cplx);
   cudaFree(p->rtw);
   cudaFree(p->rbuf);
@@ -192,56 +196,82 @@ int blue_setup(fcb_plan p, long long n, long long rows_max, int mode, bool need_
   long long m = 1;
   while (m < 2 * n - 1) m <<= 1;
   p->blue_m = m;
-  p->blue_chunk = std::max<long long>(1, std::min(rows_max, kBlueChunkSamples / m));
+  p->blue_chunk = std::max<long long>(1, std::min(rows_max, kBlueChunkSamples / n));
   for (int d = 0; d < 2; ++d)
   {
     if (!(d == 0 ? need_fwd : need_inv)) continue;
     float2 *spec = nullptr;
     rc = bluestein_tables(n, m, d == 0 ? -1 : +1, &p->chirp[d], &spec, p->stream);
     if (rc) return rc;
-    rc = fcb_plan_fastconv(m, p->blue_chunk, reinterpret_cast<const fcb_cf32 *>(spec), 1, m, FCB_REPLICA_SPECTRUM,
-                           FCB_DEVICE, &p->inner[d]);
+    rc = fcb_plan_fastconv(m, 1, reinterpret_cast<const fcb_cf32 *>(spec), 1, m, FCB_REPLICA_SPECTRUM, FCB_DEVICE,
+                           &p->inner[d]);
     cudaFree(spec);
     if (rc) return rc;
   }
-  e = cudaMalloc(&p->blue_buf[0], sizeof(float2) * (size_t)(p->blue_chunk * m));
-  if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "Bluestein work rows: %s", cudaGetErrorString(e));
+  const fcb_plan any = p->inner[0] ? p->inner[0] : p->inner[1];
+  p->kchirp = chirp_kernel(log2_exact(m), any->k->threads);
+  if (!p->kchirp) return set_error(FCB_ERR_UNSUPPORTED, "no Bluestein kernel for work rows of %lld", m);
+  rc = prepare_kernel(p->kchirp);
+  if (rc) return rc;
+  if (mode == kFastconv)
+  {
+    e = cudaMalloc(&p->blue_buf[0], sizeof(float2) * (size_t)(p->blue_chunk * n));
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "Bluestein rows: %s", cudaGetErrorString(e));
+  }
   return FCB_OK;
+}
+
+// One kChirpconv pass over `rows` rows of n samples with the tables of `inner`:
+// y = cout .* (the first n samples of IFFT_m(FFT_m(pad_m(cin .* x)) .* B) / m).
+int blue_pass(fcb_plan p, fcb_plan inner, const float2 *x, long long x_rs, float2 *y, long long y_rs, long long rows,
+              const float2 *cin, long long cin_rs, const float2 *cout, cudaStream_t st)
+{
+  RowArgs a = {};
+  a.in = x;
+  a.in_rs = x_rs;
+  a.out = y;
+  a.out_rs = y_rs;
+  a.rows = rows;
+  a.tw = a.twi = inner->tw;
+  a.rep = inner->rep;
+  a.rep_rs = 0;
+  a.scale = 1.f;
+  a.cin = cin;
+  a.cin_rs = cin_rs;
+  a.n_in = p->n;
+  a.cout = cout;
+  a.n_out = p->n;
+  a.ahead = -1;
+  return launch_rows(p->kchirp, rows, a, st);
 }
 
 int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
                 long long rows, long long row0, cudaStream_t st, int slot = 0);
 
-// Bluestein execution on stream st with work buffer `slot`, in chunks of
-// blue_chunk rows.  In place is fine: a chunk reads its input rows before it
-// writes the same rows.
+// Bluestein execution on stream st.  Fftm: one pass, chirp in and chirp *
+// scale out.  Fast convolution: a forward pass (chirp in, nothing out) into
+// rows of n, then an inverse pass (replica / n in, inverse chirp out); the
+// forward post-multiply and the inverse pre-multiply cancel (c_f c_i = 1).  In
+// place is fine: each row is read completely before it is written.
 int exec_blue(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
               long long row0, cudaStream_t st, int slot)
 {
+  if (p->mode != kFastconv)
+  {
+    const int d = p->mode == kFwd ? 0 : 1;
+    return blue_pass(p, p->inner[d], in, in_rs, out, out_rs, rows, p->chirp[d], 0, p->chirp_out, st);
+  }
   float2 *buf = p->blue_buf[slot];
-  const long long n = p->n, m = p->blue_m;
+  const long long n = p->n;
+  const bool per_row = p->rep_rows > 1;
   int rc = FCB_OK;
   for (long long r0 = 0; !rc && r0 < rows; r0 += p->blue_chunk)
   {
     const long long nr = std::min(p->blue_chunk, rows - r0);
-    const float2 *x = in + r0 * in_rs;
-    float2 *y = out + r0 * out_rs;
-    if (p->mode == kFastconv)
-    {
-      const bool per_row = p->rep_rows > 1;
-      rc = bluestein_pre(x, in_rs, p->chirp[0], buf, n, m, nr, st);
-      if (!rc) rc = exec_device(p->inner[0], buf, m, buf, m, nr, 0, st);
-      if (!rc) rc = bluestein_mid(buf, m, p->blue_rep + (per_row ? (row0 + r0) * n : 0), per_row ? n : 0, n, nr, st);
-      if (!rc) rc = exec_device(p->inner[1], buf, m, buf, m, nr, 0, st);
-      if (!rc) rc = bluestein_post(buf, m, p->chirp[1], y, out_rs, n, nr, 1.f, st);
-    }
-    else
-    {
-      const int d = p->mode == kFwd ? 0 : 1;
-      rc = bluestein_pre(x, in_rs, p->chirp[d], buf, n, m, nr, st);
-      if (!rc) rc = exec_device(p->inner[d], buf, m, buf, m, nr, 0, st);
-      if (!rc) rc = bluestein_post(buf, m, p->chirp[d], y, out_rs, n, nr, p->scale, st);
-    }
+    rc = blue_pass(p, p->inner[0], in + r0 * in_rs, in_rs, buf, n, nr, p->chirp[0], 0, nullptr, st);
+    if (!rc)
+      rc = blue_pass(p, p->inner[1], buf, n, out + r0 * out_rs, out_rs, nr,
+                     p->blue_rep + (per_row ? (row0 + r0) * n : 0), per_row ? n : 0, p->chirp[1], st);
   }
   return rc;
 }
@@ -631,6 +661,13 @@ int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale, fc
   const int mode = exponent == FCB_FORWARD ? kFwd : kInv;
   int rc = blue_length(n) ? blue_setup(p, n, rows_max, mode, mode == kFwd, mode == kInv)
                           : plan_common(p, n, rows_max, mode);
+  if (!rc && blue_length(n))
+  {
+    // the output multiplier of a Bluestein row: the chirp times the scale
+    cudaError_t e = cudaMalloc(&p->chirp_out, sizeof(float2) * (size_t)n);
+    if (e != cudaSuccess) rc = set_error(FCB_ERR_NOMEM, "Bluestein chirp: %s", cudaGetErrorString(e));
+    else rc = scale_copy(p->chirp[mode == kFwd ? 0 : 1], p->chirp_out, n, scale, p->stream);
+  }
   if (!rc)
   {
     cudaError_t e = cudaStreamSynchronize(p->stream);

@@ -9,12 +9,17 @@
 // a linear convolution of a = x .* c with b[m] = conj(c[m]), |m| < N.  With
 // M >= 2N - 1 a power of two it is the circular convolution IFFT_M(FFT_M(a) .*
 // FFT_M(b)) -- exactly what the fused kernel computes, with FFT_M(b) as its
-// "replica" spectrum (built once per plan in FP64).  A row then costs a
-// pre-multiply pass, one fused length-M pass and a post-multiply pass.
+// "replica" spectrum (built once per plan in FP64).  The pre- and
+// post-multiplies by c, the zero padding to M and the truncation to N are done
+// by the fused kernel itself in its kChirpconv mode (on its row loads and
+// stores), so a row costs one pass over its N samples.
 #include "fcb200.h"
+#include "fcb_engine.cuh"
 #include "fcb_internal.h"
 
 #include <cuda_runtime.h>
+
+#include <mutex>
 
 namespace fcb {
 
@@ -48,61 +53,6 @@ __global__ void bluestein_filter_kernel(float2 *b, long long N, long long M, int
   }
   const double2 v = chirp64(m, N, sign);
   b[i] = make_float2((float)v.x, (float)-v.y);
-}
-
-// a[r][j] = x[r][j] c[j] for j < N, 0 for N <= j < M.
-__global__ void bluestein_pre_kernel(const float2 *x, long long x_rs, const float2 *c, float2 *a, long long N,
-                                     long long M, long long rows)
-{
-  const long long total = rows * M;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x)
-  {
-    const long long r = i / M, j = i % M;
-    float2 v = make_float2(0.f, 0.f);
-    if (j < N)
-    {
-      const float2 u = x[r * x_rs + j], w = c[j];
-      v = make_float2(u.x * w.x - u.y * w.y, u.x * w.y + u.y * w.x);
-    }
-    a[i] = v;
-  }
-}
-
-// out[r][k] = scale * c[k] * y[r][k], k < N.
-__global__ void bluestein_post_kernel(const float2 *y, long long M, const float2 *c, float2 *out, long long out_rs,
-                                      long long N, long long rows, float scale)
-{
-  const long long total = rows * N;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x)
-  {
-    const long long r = i / N, k = i % N;
-    const float2 u = y[r * M + k], w = c[k];
-    out[r * out_rs + k] = make_float2(scale * (u.x * w.x - u.y * w.y), scale * (u.x * w.y + u.y * w.x));
-  }
-}
-
-// Fast convolution between the two Bluestein passes: the forward pass's
-// post-multiply by c and the inverse pass's pre-multiply by conj(c) cancel
-// (|c| = 1), leaving y[r][k] = R[r][k] y[r][k] for k < N and 0 beyond.
-// rep holds R / N (rep_rs 0: one row for all).
-__global__ void bluestein_mid_kernel(float2 *y, long long M, const float2 *rep, long long rep_rs, long long N,
-                                     long long rows)
-{
-  const long long total = rows * M;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-       i += (long long)gridDim.x * blockDim.x)
-  {
-    const long long r = i / M, k = i % M;
-    float2 v = make_float2(0.f, 0.f);
-    if (k < N)
-    {
-      const float2 u = y[i], w = rep[r * rep_rs + k];
-      v = make_float2(u.x * w.x - u.y * w.y, u.x * w.y + u.y * w.x);
-    }
-    y[i] = v;
-  }
 }
 
 __global__ void scale_kernel(const float2 *in, float2 *out, long long total, float s)
@@ -140,35 +90,51 @@ int bluestein_tables(long long N, long long M, int sign, float2 **chirp, float2 
   return FCB_OK;
 }
 
-int bluestein_pre(const float2 *x, long long x_rs, const float2 *c, float2 *a, long long N, long long M,
-                  long long rows, cudaStream_t st)
-{
-  bluestein_pre_kernel<<<grid_for(rows * M), 256, 0, st>>>(x, x_rs, c, a, N, M, rows);
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? FCB_OK : cuda_error(e, "Bluestein pre-multiply");
-}
-
-int bluestein_post(const float2 *y, long long M, const float2 *c, float2 *out, long long out_rs, long long N,
-                   long long rows, float scale, cudaStream_t st)
-{
-  bluestein_post_kernel<<<grid_for(rows * N), 256, 0, st>>>(y, M, c, out, out_rs, N, rows, scale);
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? FCB_OK : cuda_error(e, "Bluestein post-multiply");
-}
-
-int bluestein_mid(float2 *y, long long M, const float2 *rep, long long rep_rs, long long N, long long rows,
-                  cudaStream_t st)
-{
-  bluestein_mid_kernel<<<grid_for(rows * M), 256, 0, st>>>(y, M, rep, rep_rs, N, rows);
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? FCB_OK : cuda_error(e, "Bluestein replica multiply");
-}
-
 int scale_copy(const float2 *in, float2 *out, long long total, float s, cudaStream_t st)
 {
   scale_kernel<<<grid_for(total), 256, 0, st>>>(in, out, total, s);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FCB_OK : cuda_error(e, "scale copy");
+}
+
+// Kernel table of the kChirpconv mode: work rows of 8 .. 65536 samples, the
+// same CTA-size variants as the other modes ([0] 256, [1] 512, [2] 128 threads).
+template <int LOGN, int T>
+static KernelInfo chirp_info()
+{
+  using S = Sched<LOGN, T>;
+  KernelInfo k;
+  k.fn = (const void *)&rows_kernel<LOGN, kChirpconv, T>;
+  k.threads = T;
+  k.cluster = S::CS;
+  k.rows_per_cta = S::ROWS;
+  k.smem = S::SMEM;
+  k.tw_bytes = S::tw_bytes();
+  return k;
+}
+
+template <int LOGN>
+static void fill_chirp(KernelInfo (*tab)[3])
+{
+  if constexpr (LOGN >= 3)
+  {
+    tab[LOGN][0] = chirp_info<LOGN, 256>();
+    if constexpr (LOGN >= kMin512) tab[LOGN][1] = chirp_info<LOGN, 512>();
+    if constexpr (LOGN >= kMin128 && LOGN <= kMax128) tab[LOGN][2] = chirp_info<LOGN, 128>();
+    fill_chirp<LOGN - 1>(tab);
+  }
+}
+
+static KernelInfo g_chirp[kMaxLogN + 1][3];
+static std::once_flag g_chirp_once;
+
+const KernelInfo *chirp_kernel(int logn, int threads)
+{
+  std::call_once(g_chirp_once, [] { fill_chirp<kMaxLogN>(g_chirp); });
+  if (logn < 3 || logn > kMaxLogN) return nullptr;
+  const int v = (threads == 512 && logn >= kMin512) ? 1
+              : (threads == 128 && logn >= kMin128 && logn <= kMax128) ? 2 : 0;
+  return &g_chirp[logn][v];
 }
 
 }  // namespace fcb

@@ -242,6 +242,13 @@ __device__ __forceinline__ float4 ldv4(const float4 *p)
   return v;
 }
 
+__device__ __forceinline__ float2 ldv2(const float2 *p)
+{
+  float2 v;
+  asm volatile("ld.global.nc.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+  return v;
+}
+
 // Shared-memory access through 32-bit addresses.  In a cluster, peer CTAs'
 // slots are reached through their shared::cluster window (mapa); a CTA's own
 // shared::cta address is used for its own slots.
@@ -322,6 +329,14 @@ struct RowArgs
   long long ahead;      // L2 prefetch distance in tiles (CTAs, or clusters) -- about
                         // half a resident wave, so that tile's rows stream from
                         // HBM into L2 while this tile computes; 0 = off
+  // kChirpconv only (Bluestein rows, whose n samples sit in power-of-two work
+  // rows): the row is read as in[k] * cin[row * cin_rs + k] for k < n_in and
+  // 0 beyond, and written for k < n_out only, times cout[k] when cout is set.
+  const float2 *cin;
+  long long cin_rs;
+  long long n_in;
+  const float2 *cout;
+  long long n_out;
 };
 
 __device__ __forceinline__ void prefetch_l2(const void *p)
@@ -329,7 +344,14 @@ __device__ __forceinline__ void prefetch_l2(const void *p)
   asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
 }
 
-enum Mode { kFwd = 0, kInv = 1, kFastconv = 2 };
+// kChirpconv is the fused fast convolution with element-wise multipliers and
+// zero padding on the way in and truncation on the way out (Bluestein rows).
+enum Mode { kFwd = 0, kInv = 1, kFastconv = 2, kChirpconv = 3 };
+
+__device__ __forceinline__ float2 c_mul(float2 a, float2 b)
+{
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
 
 // Where a slot of the row lives: owning cluster rank and CTA-local index.
 template <class S>
@@ -381,6 +403,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 {
   using S = Sched<LOGN, THREADS>;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
+  constexpr bool CHIRP = MODE == kChirpconv;
+  constexpr int MD = CHIRP ? kFastconv : MODE;    // the transform structure
   constexpr int LH1 = ilog2(S::H1);
   constexpr bool CL = S::CS > 1;
   extern __shared__ float4 smem[];
@@ -425,9 +449,33 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   {
     float2 x[S::EPT];
     const float2 *src = a.in + row * a.in_rs;
+    if constexpr (CHIRP)
+    {
+      // samples and multipliers in batches of eight (both at once would double
+      // the live registers); the multiplier loads stay in place (volatile)
+      const float2 *mul = a.cin + (active ? row : 0) * a.cin_rs;
 #pragma unroll
-    for (int j = 0; j < S::EPT; ++j)
-      x[j] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
+      for (int j0 = 0; j0 < S::EPT; j0 += 8)
+      {
+        float2 m[8];
+#pragma unroll
+        for (int j = j0; j < j0 + 8 && j < S::EPT; ++j)
+        {
+          const int k = tr + S::TPR * j;
+          const bool in = active && k < a.n_in;
+          x[j] = in ? __ldg(src + k) : make_float2(0.f, 0.f);
+          m[j - j0] = in ? ldv2(mul + k) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int j = j0; j < j0 + 8 && j < S::EPT; ++j) x[j] = c_mul(x[j], m[j - j0]);
+      }
+    }
+    else
+    {
+#pragma unroll
+      for (int j = 0; j < S::EPT; ++j)
+        x[j] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
+    }
     // With this tile's loads in flight, prefetch into L2 the input of the tile
     // `ahead` tiles later (about half a resident wave), so that it streams in
     // from HBM while this tile computes.  Straight-line code (a few lines per
@@ -443,7 +491,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         const int i = t + THREADS * k;
         const int li = rank * LINES + i;
         const long long r = row0 + li / LPR;
-        if (a.ahead > 0 && i < LINES && r < a.rows) prefetch_l2(a.in + r * a.in_rs + (li % LPR) * 16);
+        if (a.ahead > 0 && i < LINES && r < a.rows && (!CHIRP || (li % LPR) * 16 < a.n_in))
+          prefetch_l2(a.in + r * a.in_rs + (li % LPR) * 16);
       }
     }
     // W_N^{tr q} for q = 2q' + lane; groups g > 0 add the constant W_32^{g q}
@@ -508,7 +557,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     for (int r = 0; r < 16; ++r)
       c[r] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * r, rho))));
     float4 ra[4];  // replica entries, four at a time
-    if constexpr (MODE == kFastconv && s == S::NS)
+    if constexpr (MD == kFastconv && s == S::NS)
     {
 #pragma unroll
       for (int i = 0; i < 4; ++i) ra[i] = ldv4(rp + i * S::TPR + tr);
@@ -534,7 +583,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         }
       }
     }
-    if constexpr (MODE == kFastconv && s == S::NS)
+    if constexpr (MD == kFastconv && s == S::NS)
     {
 #pragma unroll
       for (int b = 0; b < 16; b += 4)
@@ -560,7 +609,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   if constexpr (S::NS >= 3) stage_fwd(ic<3>{});
   if constexpr (S::NS >= 4) stage_fwd(ic<4>{});
 
-  if constexpr (MODE != kFastconv)
+  if constexpr (MD != kFastconv)
   {
     // ---------------- reorder to natural frequency order and store ----------------
     // c[] holds the last stage's outputs (never written back).  Pair slot
@@ -758,7 +807,18 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         if (k == 0) { tr_ = br; ti_ = bi; }
         else if (k == 8) { tr_ = -bi; ti_ = br; }
         else { tr_ = fmaf(br, wc, -bi * ws); ti_ = fmaf(br, ws, bi * wc); }
-        if (active)
+        if constexpr (CHIRP)
+        {
+          // only the first n_out samples of the work row are wanted
+          const int c0 = tr + S::TPR * g + S::D * r, c1 = c0 + S::D * S::H1;
+          const float2 v0 = make_float2(ar + tr_, ai + ti_), v1 = make_float2(ar - tr_, ai - ti_);
+          // multiplier loads stay next to their use (volatile), not hoisted
+          if (active && c0 < a.n_out)
+            dst_t[S::TPR * g + S::D * r] = a.cout ? c_mul(v0, ldv2(a.cout + c0)) : v0;
+          if (active && c1 < a.n_out)
+            dst_t[S::TPR * g + S::D * (r + S::H1)] = a.cout ? c_mul(v1, ldv2(a.cout + c1)) : v1;
+        }
+        else if (active)
         {
           dst_t[S::TPR * g + S::D * r] = make_float2(ar + tr_, ai + ti_);
           dst_t[S::TPR * g + S::D * (r + S::H1)] = make_float2(ar - tr_, ai - ti_);

@@ -26,7 +26,13 @@ struct KernelInfo
   long long resident_tiles = 0;  // CTAs (or clusters) resident at once, set by prepare_kernel
 };
 
+constexpr int kMin512 = 12;  // 512-thread variants exist for rows of 4096 samples and more
+constexpr int kMin128 = 8, kMax128 = 14;  // 128-thread variants: rows of 256 .. 16384 samples
+
 const KernelInfo *kernel_info(int logn, int mode);
+// Fused kernel with element-wise multipliers (kChirpconv, fcb_bluestein.cu)
+// for work rows of 2^logn samples, CTA size as close to `threads` as exists.
+const KernelInfo *chirp_kernel(int logn, int threads);
 int set_variant(int logn, int mode, int threads);
 const KernelInfo *kernel_variant(int logn, int mode, int threads);
 int get_variant(int logn, int mode);
@@ -46,12 +52,6 @@ int launch_scale_rows(const float2 *in, long long in_rs, float2 *out, long long 
 // Bluestein chirp-z pieces (fcb_bluestein.cu) for rows of non-power-of-two
 // length N, computed through power-of-two work rows of M >= 2N - 1 samples.
 int bluestein_tables(long long N, long long M, int sign, float2 **chirp, float2 **spectrum, cudaStream_t st);
-int bluestein_pre(const float2 *x, long long x_rs, const float2 *c, float2 *a, long long N, long long M,
-                  long long rows, cudaStream_t st);
-int bluestein_post(const float2 *y, long long M, const float2 *c, float2 *out, long long out_rs, long long N,
-                   long long rows, float scale, cudaStream_t st);
-int bluestein_mid(float2 *y, long long M, const float2 *rep, long long rep_rs, long long N, long long rows,
-                  cudaStream_t st);
 int scale_copy(const float2 *in, float2 *out, long long total, float s, cudaStream_t st);
 
 // Real-input row FFTs (fcb_real.cu).
