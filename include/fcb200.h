@@ -91,17 +91,17 @@ FCB_API const char *fcb_version(void);
 FCB_API int fcb_init(int device);
 /* 1 if n is a supported row length for Fftm and fast-convolution plans: any
  * length in [1, 32768], or a power of two up to 65536.  Powers of two run as
- * one fused pass; other lengths by Bluestein's chirp-z algorithm over work
- * rows of the next power of two >= 2n - 1 samples (a chirp pre-multiply, one
- * fused pass per transform, a chirp post-multiply).  The reference's FFTW
+ * one fused pass; other lengths by Bluestein's chirp-z algorithm: the fused
+ * kernel runs on work rows of the next power of two >= 2n - 1 samples and
+ * applies the chirps, the zero padding and the truncation to n samples on its
+ * own loads and stores (one pass per transform).  The reference's FFTW
  * backend plans any length (src/ovxx/fftw/fftw.cpp:39-116). */
 FCB_API int fcb_supported_length(long long n);
 
 /* Row-wise multiple FFT plan: n samples per row, up to rows_max rows per call,
  * exponent FCB_FORWARD or FCB_INVERSE, output multiplied by scale.  Replaces
  * fftm_backend<complex<float>, complex<float>, 0, D> (src/ovxx/signal/fft/
- * backend.hpp:696-784; FFTW plan src/ovxx/fftw/fftw.cpp:904-1001).  A
- * non-power-of-two plan keeps a work buffer of at most 2^25 samples. */
+ * backend.hpp:696-784; FFTW plan src/ovxx/fftw/fftw.cpp:904-1001). */
 FCB_API int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale,
                   fcb_plan *plan);
 
