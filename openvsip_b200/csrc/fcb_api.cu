@@ -379,6 +379,21 @@ int exec_real_device(fcb_plan p, const void *in, long long in_rs, void *out, lon
   return rc;
 }
 
+// A host-buffer call returns only once none of its copies is queued or running,
+// on an error too: its caller may free or reuse the host buffers as soon as
+// the call returns.  Waits for the plan's streams and keeps the first error.
+int host_done(fcb_plan p, int rc, const char *what)
+{
+  const cudaStream_t ss[3] = {p->cin, p->cout, p->stream};
+  for (int i = 0; i < 3; ++i)
+  {
+    if (i < 2 && !ss[i]) continue;  // copy streams not created yet (the plan stream may be NULL: default stream)
+    const cudaError_t e = cudaStreamSynchronize(ss[i]);
+    if (e != cudaSuccess && rc == FCB_OK) rc = cuda_error(e, what);
+  }
+  return rc;
+}
+
 // Real-input rows on host pointers: chunks staged through two device buffers.
 int exec_real_host(fcb_plan p, const void *in, long long in_rs, void *out, long long out_rs, long long rows)
 {
@@ -409,16 +424,15 @@ int exec_real_host(fcb_plan p, const void *in, long long in_rs, void *out, long 
     cudaError_t e = cudaMemcpy2DAsync(p->rstage[0], in_el * (size_t)in_pitch, src + in_el * (size_t)(r0 * in_rs),
                                       in_el * (size_t)in_rs, in_el * (size_t)in_cols, (size_t)nr,
                                       cudaMemcpyHostToDevice, p->stream);
-    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "real FFT (host)");
     int rc = exec_real_device(p, p->rstage[0], in_pitch, p->rstage[1], out_pitch, nr, p->stream);
-    if (rc) return rc;
+    if (rc) return host_done(p, rc, "real FFT (host)");
     e = cudaMemcpy2DAsync(dst + out_el * (size_t)(r0 * out_rs), out_el * (size_t)out_rs, p->rstage[1],
                           out_el * (size_t)out_pitch, out_el * (size_t)out_cols, (size_t)nr,
                           cudaMemcpyDeviceToHost, p->stream);
-    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "real FFT (host)");
   }
-  cudaError_t e = cudaStreamSynchronize(p->stream);
-  return e == cudaSuccess ? FCB_OK : cuda_error(e, "real FFT (host)");
+  return host_done(p, FCB_OK, "real FFT (host)");
 }
 
 int exec_real(fcb_plan p, int kind, const void *in, long long in_rs, void *out, long long out_rs, long long rows,
@@ -596,27 +610,21 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
                       ? cudaMemcpyAsync(buf, in + r0 * in_rs, row_bytes * (size_t)nr, cudaMemcpyHostToDevice, p->cin)
                       : cudaMemcpy2DAsync(buf, row_bytes, in + r0 * in_rs, sizeof(float2) * (size_t)in_rs, row_bytes,
                                           (size_t)nr, cudaMemcpyHostToDevice, p->cin);
-    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "fcb_exec (host)");
     cudaEventRecord(p->ev_in[b], p->cin);
     cudaStreamWaitEvent(p->stream, p->ev_in[b], 0);
     rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, p->stream, 0);
-    if (rc) return rc;
+    if (rc) return host_done(p, rc, "fcb_exec (host)");
     cudaEventRecord(p->ev_k[b], p->stream);
     cudaStreamWaitEvent(p->cout, p->ev_k[b], 0);
     e = out_rs == p->n
           ? cudaMemcpyAsync(out + r0 * out_rs, buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
           : cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,
                               (size_t)nr, cudaMemcpyDeviceToHost, p->cout);
-    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "fcb_exec (host)");
     cudaEventRecord(p->ev_out[b], p->cout);
   }
-  cudaError_t e1 = cudaStreamSynchronize(p->cout);
-  cudaError_t e2 = cudaStreamSynchronize(p->stream);
-  cudaError_t e3 = cudaStreamSynchronize(p->cin);
-  if (e1 != cudaSuccess) return cuda_error(e1, "fcb_exec (host)");
-  if (e2 != cudaSuccess) return cuda_error(e2, "fcb_exec (host)");
-  if (e3 != cudaSuccess) return cuda_error(e3, "fcb_exec (host)");
-  return FCB_OK;
+  return host_done(p, FCB_OK, "fcb_exec (host)");
 }
 
 }  // namespace
@@ -793,15 +801,13 @@ int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, lon
     const size_t rb = sizeof(float2) * (size_t)p->cols2d;
     e = cudaMemcpy2DAsync(p->stage2d_in, rb, i2, sizeof(float2) * (size_t)in_rs, rb, (size_t)p->rows2d,
                           cudaMemcpyHostToDevice, p->stream);
-    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "fcb_exec (2-D, host)");
     int rc = exec_2d(p, p->stage2d_in, p->cols2d, p->stage2d_in, p->cols2d, p->stream);
-    if (rc) return rc;
+    if (rc) return host_done(p, rc, "fcb_exec (2-D, host)");
     e = cudaMemcpy2DAsync(o2, sizeof(float2) * (size_t)out_rs, p->stage2d_in, rb, rb, (size_t)p->rows2d,
                           cudaMemcpyDeviceToHost, p->stream);
-    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
-    e = cudaStreamSynchronize(p->stream);
-    if (e != cudaSuccess) return cuda_error(e, "fcb_exec (2-D, host)");
-    return FCB_OK;
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "fcb_exec (2-D, host)");
+    return host_done(p, FCB_OK, "fcb_exec (2-D, host)");
   }
   if (where == FCB_DEVICE) return exec_device(p, i2, in_rs, o2, out_rs, rows, 0, p->stream);
   return exec_host(p, i2, in_rs, o2, out_rs, rows);
