@@ -66,6 +66,8 @@ def _desc(x, writable: bool, real: bool = False):
         raise TypeError("expected a numpy float32 array" if real else "expected a numpy complex64 array")
     if a.ndim == 1:
         a = a.reshape(1, -1)
+    if a.ndim == 2 and a.size == 0:  # empty: numpy reports zero strides, nothing is accessed
+        return a.ctypes.data, a.shape[0], a.shape[1], max(1, a.shape[1]), _lib.FCB_HOST
     if a.ndim != 2 or (a.shape[1] > 1 and a.strides[1] != el) or a.strides[0] % el:
         raise ValueError("expected a 2-D array with unit-stride rows")
     if writable and not a.flags.writeable:

@@ -76,3 +76,11 @@ def test_python_api_validates_types():
         signal._desc(np.zeros((2, 4, 2), dtype=np.complex64), False)
     ptr, r, c, rs, where = signal._desc(np.zeros((3, 8), dtype=np.complex64)[:, :4], False)
     assert (r, c, rs, where) == (3, 4, 8, _lib.FCB_HOST)
+
+
+def test_empty_arrays_are_described_without_strides():
+    # numpy reports zero strides for empty arrays; an empty call must still pass
+    import numpy as np
+    from openvsip_b200.vsip import _desc
+    assert _desc(np.zeros((0, 1024), dtype=np.complex64), False)[1:] == (0, 1024, 1024, 0)
+    assert _desc(np.zeros((0, 16), dtype=np.float32), False, real=True)[1:] == (0, 16, 16, 0)
