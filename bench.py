@@ -564,7 +564,8 @@ def main():
                        "l2": f"inputs larger than L2 ({16 * samples_step >> 20} MB read+write per step, "
                              "2 alternating inputs)",
                        "kernel": {"threads": info["threads"], "cluster_ctas": info["cluster_ctas"],
-                                  "smem_bytes": info["smem_bytes"]}},
+                                  "smem_bytes": info["smem_bytes"],
+                                  "variant": int(ov.lib().fcb_tune_get(nsamp, 2))}},
             "latency_ms": {"p50": sorted_ms[len(sorted_ms) // 2],
                            "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))]},
             "rel_l2_vs_fp64": rel,

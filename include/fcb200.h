@@ -162,13 +162,15 @@ FCB_API int fcb_destroy(fcb_plan plan);
 FCB_API int fcb_plan_info(fcb_plan plan, long long *n, int *cluster_ctas,
                   int *rows_per_cta, int *smem_bytes, int *threads);
 
-/* Kernel variant for row length n and kind (FCB_KIND_*): CTAs of 256 or 512
- * threads.  Set by the autotuner; applies to plans created afterwards.
- * No reference counterpart (FFTW's planning rigor, src/ovxx/fftw/fft.cpp:44-52,
- * is the closest analogue). */
+/* Kernel variant for row length n and kind (FCB_KIND_*): CTAs of 128, 256 or
+ * 512 threads with 32 samples per thread (128: rows of 256 .. 8192 samples;
+ * 512: 4096 and more), or -256: CTAs of 256 threads with 64 samples per thread
+ * (rows of 16384 samples; one stage fewer).  Set by the autotuner; applies to
+ * plans created afterwards.  No reference counterpart (FFTW's planning rigor,
+ * src/ovxx/fftw/fft.cpp:44-52, is the closest analogue). */
 enum fcb_kind { FCB_KIND_FORWARD = 0, FCB_KIND_INVERSE = 1, FCB_KIND_FASTCONV = 2 };
 FCB_API int fcb_tune_set(long long n, int kind, int threads);
-/* Current variant (256 or 512) for n and kind, 0 if n has none. */
+/* Current variant (128, 256, 512 or -256) for n and kind, 0 if n has none. */
 FCB_API int fcb_tune_get(long long n, int kind);
 
 /* out[r][c] = v[c] * m[r][c] on the device (asynchronous on `stream`). */

@@ -4,9 +4,10 @@ What it chooses (measured on the device with CUDA events, never guessed):
 
 * For each row length and kind (forward Fftm, inverse Fftm, fused fastconv),
   the tile schedule of the row kernel: CTAs of 128 threads (4096 samples per
-  CTA, four CTAs per SM; rows of 256 .. 16384 samples), 256 threads (8192
+  CTA, four CTAs per SM; rows of 256 .. 8192 samples), 256 threads (8192
   samples, two per SM) or 512 threads (16384 samples, one per SM; rows of 4096
-  samples and more).  Rows longer than one CTA's samples split over a
+  samples and more), or 256 threads with 64 samples each (value -256, rows of
+  16384 samples).  Rows longer than one CTA's samples split over a
   thread-block cluster.  The choice is installed with fcb_tune_set and applies
   to plans made afterwards.
 * For the batched launch: the same CTA size (which also fixes the cluster
@@ -30,12 +31,15 @@ VARIANT_MIN_N = 256  # below this every length has only the 256-thread kernel
 
 
 def variants(n: int) -> tuple:
-    """CTA sizes the library has kernels for at row length n."""
+    """Kernel variants the library has at row length n: CTA sizes with 32
+    samples per thread, and -256 (256 threads x 64 samples) at 16384."""
     out = [256]
-    if 256 <= n <= 16384:
+    if 256 <= n <= 8192:
         out.insert(0, 128)
     if n >= 4096:
         out.append(512)
+    if n == 16384:
+        out.append(-256)
     return tuple(out)
 
 

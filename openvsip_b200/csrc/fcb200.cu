@@ -38,17 +38,20 @@ int cuda_error(cudaError_t e, const char *what)
 
 // ---------------------------------------------------------------------------
 // Runtime view of the compile-time schedule (for table builders).
-SchedRT sched_rt(int logn)
+SchedRT sched_rt(int logn, int ept)
 {
   SchedRT s;
   s.logn = logn;
   s.n = 1 << logn;
-  s.ns = (logn <= 5) ? 1 : 1 + (logn - 5 + 3) / 4;
-  s.r1 = 1 << (logn - 4 * (s.ns - 1));
+  s.ept = ept;
+  s.rb = ept / 2;
+  s.lrb = ept == 64 ? 5 : 4;
+  s.ns = (logn <= s.lrb + 1) ? 1 : 1 + (logn - (s.lrb + 1) + s.lrb - 1) / s.lrb;
+  s.r1 = 1 << (logn - s.lrb * (s.ns - 1));
   s.d = s.n / s.r1;
   s.half = s.n / 2;
   s.tw2_size = 0;
-  for (int k = 2; k <= s.ns; ++k) s.tw2_size += s.d >> (4 * (k - 2));
+  for (int k = 2; k <= s.ns; ++k) s.tw2_size += s.d >> (s.lrb * (k - 2));
   return s;
 }
 
@@ -74,7 +77,7 @@ __global__ void build_tw_kernel(float4 *tw, SchedRT s)
   long long off = 0;
   for (int k = 2; k <= s.ns; ++k)
   {
-    long long L = s.d >> (4 * (k - 2)), St = L / 16;
+    long long L = s.d >> (s.lrb * (k - 2)), St = L / s.rb;
     if (j < off + L)
     {
       long long jj = j - off, q = jj / St, n = jj % St;
@@ -89,11 +92,11 @@ __global__ void build_tw_kernel(float4 *tw, SchedRT s)
 }
 
 // Replica pair table, (R[k]/N, R[k+1]/N) split per entry (1/N is exact).
-// Slot sigma = q'*D + P holds the pair k = 2q' + R1 * digitrev16(P).  Rows of
+// Slot sigma = q'*D + P holds the pair k = 2q' + R1 * digitrev_RB(P).  Rows of
 // one stage keep slot order.  Multi-stage rows use the order in which the
-// last stage reads: there thread tr of a row (TPR = N/32 threads) owns slots
-// 16 tr .. 16 tr + 15 and multiplies its i-th value by slot 16 tr +
-// bitrev4(i), so entry i * TPR + tr holds that slot and the i-th loads of a
+// last stage reads: there thread tr of a row (TPR = N/EPT threads) owns slots
+// RB tr .. RB tr + RB - 1 and multiplies its i-th value by slot RB tr +
+// bitrev(i), so entry i * TPR + tr holds that slot and the i-th loads of a
 // warp read consecutive entries (one coalesced 512-byte access).
 __global__ void build_rep_kernel(const float2 *spec, long long spec_rs, float4 *rep,
                                  long long rows, SchedRT s)
@@ -105,11 +108,11 @@ __global__ void build_rep_kernel(const float2 *spec, long long spec_rs, float4 *
   long long sigma = e;
   if (s.ns > 1)
   {
-    const long long tpr = s.n / 32, j = e / tpr, tr = e % tpr;
-    sigma = 16 * tr + bitrev((int)j, 4);
+    const long long tpr = s.n / s.ept, j = e / tpr, tr = e % tpr;
+    sigma = s.rb * tr + bitrev((int)j, s.lrb);
   }
   int qp = (int)(sigma / s.d), P = (int)(sigma % s.d);
-  int k = 2 * qp + s.r1 * digitrev16(P, s.ns - 1);
+  int k = 2 * qp + s.r1 * digitrev16(P, s.ns - 1, s.lrb);
   const float inv = 1.0f / (float)s.n;
   float2 a = spec[r * spec_rs + k], b = spec[r * spec_rs + k + 1];
   rep[i] = make_float4(a.x * inv, b.x * inv, a.y * inv, b.y * inv);
@@ -217,12 +220,13 @@ __global__ void scale_rows_kernel(const float2 *in, long long in_rs, float2 *out
 
 // ---------------------------------------------------------------------------
 // Kernel table: [logn][mode][variant], variant 0 = 256-thread CTAs, 1 = 512.
-template <int LOGN, int MODE, int T>
+template <int LOGN, int MODE, int T, int EPTW = 32>
 static KernelInfo make_info()
 {
-  using S = Sched<LOGN, T>;
+  using S = Sched<LOGN, T, EPTW>;
   KernelInfo k;
-  k.fn = (const void *)&rows_kernel<LOGN, MODE, T>;
+  k.fn = (const void *)&rows_kernel<LOGN, MODE, T, EPTW>;
+  k.ept = EPTW;
   k.threads = T;
   k.cluster = S::CS;
   k.rows_per_cta = S::ROWS;
@@ -233,7 +237,7 @@ static KernelInfo make_info()
 
 
 template <int LOGN>
-static void fill_table(KernelInfo (*tab)[3][3])
+static void fill_table(KernelInfo (*tab)[3][kVariants])
 {
   if constexpr (LOGN >= 1)
   {
@@ -252,11 +256,17 @@ static void fill_table(KernelInfo (*tab)[3][3])
       tab[LOGN][kInv][2] = make_info<LOGN, kInv, 128>();
       tab[LOGN][kFastconv][2] = make_info<LOGN, kFastconv, 128>();
     }
+    if constexpr (LOGN == kWideLog)
+    {
+      tab[LOGN][kFwd][3] = make_info<LOGN, kFwd, 256, 64>();
+      tab[LOGN][kInv][3] = make_info<LOGN, kInv, 256, 64>();
+      tab[LOGN][kFastconv][3] = make_info<LOGN, kFastconv, 256, 64>();
+    }
     fill_table<LOGN - 1>(tab);
   }
 }
 
-static KernelInfo g_table[kMaxLogN + 1][3][3];
+static KernelInfo g_table[kMaxLogN + 1][3][kVariants];
 static std::once_flag g_table_once;
 // Variant chosen per (logn, mode); set by the autotuner through fcb_tune_set.
 static int g_variant[kMaxLogN + 1][3];
@@ -271,8 +281,10 @@ static void init_table()
         // defaults (measured): 4 CTAs of 128 threads per SM for rows of 256 ..
         // 4096 samples, 256-thread CTAs for 8192, 512-thread CTAs from 16384
         // up (clusters of 2 and 4 of them for 32768 and 65536; clusters of
-        // smaller CTAs measured slower at every length)
-        g_variant[l][m] = (l >= 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
+        // smaller CTAs measured slower at every length), except the fused
+        // fast convolution of 16384-sample rows: the wide variant (one stage,
+        // two slot exchanges fewer), 13 % faster
+        g_variant[l][m] = (l == kWideLog && m == kFastconv) ? 3 : (l >= 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
   });
 }
 
@@ -284,13 +296,23 @@ const KernelInfo *kernel_info(int logn, int mode)
   return &g_table[logn][mode][g_variant[logn][mode]];
 }
 
+// Public tuning values: 128, 256, 512 threads (32 samples per thread), or -256
+// for the wide variant (256 threads x 64 samples).
+static int variant_id(int logn, int threads)
+{
+  if (threads == -256 && logn == kWideLog) return 3;
+  if (threads == 512 && logn >= kMin512) return 1;
+  if (threads == 128 && logn >= kMin128 && logn <= kMax128) return 2;
+  return threads == 256 ? 0 : -1;
+}
+static const int kVariantValue[kVariants] = {256, 512, 128, -256};
+
 const KernelInfo *kernel_variant(int logn, int mode, int threads)
 {
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return nullptr;
-  const int v = (threads == 512 && logn >= kMin512) ? 1
-              : (threads == 128 && logn >= kMin128 && logn <= kMax128) ? 2 : 0;
-  return &g_table[logn][mode][v];
+  const int v = variant_id(logn, threads);
+  return &g_table[logn][mode][v < 0 ? 0 : v];
 }
 
 int set_variant(int logn, int mode, int threads)
@@ -298,11 +320,12 @@ int set_variant(int logn, int mode, int threads)
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2)
     return set_error(FCB_ERR_INVALID, "bad length or mode for tuning");
-  int v = threads == 512 ? 1 : threads == 256 ? 0 : threads == 128 ? 2 : -1;
-  if (v < 0) return set_error(FCB_ERR_INVALID, "threads must be 128, 256 or 512");
-  if (v == 1 && logn < kMin512) return set_error(FCB_ERR_UNSUPPORTED, "no 512-thread variant below 4096 samples");
-  if (v == 2 && (logn < kMin128 || logn > kMax128))
-    return set_error(FCB_ERR_UNSUPPORTED, "128-thread variants exist for 256 .. 16384 samples");
+  if (threads != 128 && threads != 256 && threads != 512 && threads != -256)
+    return set_error(FCB_ERR_INVALID, "threads must be 128, 256, 512 or -256 (wide)");
+  const int v = variant_id(logn, threads);
+  if (v < 0)
+    return set_error(FCB_ERR_UNSUPPORTED, "no %d-thread variant for rows of %d samples (512: 4096 and more; "
+                     "128: 256 .. 8192; -256: 16384)", threads, 1 << logn);
   std::lock_guard<std::mutex> lk(g_variant_mu);
   g_variant[logn][mode] = v;
   return FCB_OK;
@@ -313,7 +336,7 @@ int get_variant(int logn, int mode)
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return 0;
   std::lock_guard<std::mutex> lk(g_variant_mu);
-  return g_variant[logn][mode] == 1 ? 512 : g_variant[logn][mode] == 2 ? 128 : 256;
+  return kVariantValue[g_variant[logn][mode]];
 }
 
 int prepare_kernel(const KernelInfo *k)
@@ -359,9 +382,9 @@ int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaSt
   return FCB_OK;
 }
 
-int build_twiddles(int logn, float4 **out, cudaStream_t st)
+int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st)
 {
-  SchedRT s = sched_rt(logn);
+  SchedRT s = sched_rt(logn, ept);
   float4 *tw = nullptr;
   const size_t bytes = 16 * (size_t)s.half + 8 * (size_t)s.tw2_size;
   cudaError_t e = cudaMalloc(&tw, bytes);
@@ -374,10 +397,10 @@ int build_twiddles(int logn, float4 **out, cudaStream_t st)
   return FCB_OK;
 }
 
-int build_replica_table(int logn, const float2 *spec_dev, long long spec_rs, long long rows,
+int build_replica_table(int logn, int ept, const float2 *spec_dev, long long spec_rs, long long rows,
                         float4 *rep_dev, cudaStream_t st)
 {
-  SchedRT s = sched_rt(logn);
+  SchedRT s = sched_rt(logn, ept);
   long long total = rows * s.half;
   build_rep_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(spec_dev, spec_rs, rep_dev, rows, s);
   cudaError_t e = cudaGetLastError();

@@ -173,7 +173,7 @@ int plan_common(fcb_plan p, long long n, long long rows_max, int mode)
     p->k = kernel_info(p->logn, mode);
     rc = prepare_kernel(p->k);
     if (rc) return rc;
-    rc = build_twiddles(p->logn, &p->tw, p->stream);
+    rc = build_twiddles(p->logn, p->k->ept, &p->tw, p->stream);
     if (rc) return rc;
   }
   return FCB_OK;
@@ -209,7 +209,7 @@ int blue_setup(fcb_plan p, long long n, long long rows_max, int mode, bool need_
     if (rc) return rc;
   }
   const fcb_plan any = p->inner[0] ? p->inner[0] : p->inner[1];
-  p->kchirp = chirp_kernel(log2_exact(m), any->k->threads);
+  p->kchirp = chirp_kernel(log2_exact(m), any->k);
   if (!p->kchirp) return set_error(FCB_ERR_UNSUPPORTED, "no Bluestein kernel for work rows of %lld", m);
   rc = prepare_kernel(p->kchirp);
   if (rc) return rc;
@@ -742,7 +742,7 @@ int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, 
       if (!rc)
       {
         if (p->logn >= 1)
-          rc = build_replica_table(p->logn, spec, n, replica_rows, p->rep, p->stream);
+          rc = build_replica_table(p->logn, p->k->ept, spec, n, replica_rows, p->rep, p->stream);
         else
         {
           // length 1: table entry (R.re, -, R.im, -)
@@ -924,11 +924,19 @@ int fcb_plan_fft2d(long long rows, long long cols, int exponent, float scale, fc
   {
     // 512-thread CTAs hold 4 rows of 4096 (or more of shorter rows), so each
     // transposed store writes whole 32-byte sectors
+    const int built_ept = p->k->ept;
     p->k = kernel_variant(lc, mode, 512);
     p->kc = kernel_variant(lr, mode, 512);
     rc = prepare_kernel(p->k);
     if (!rc) rc = prepare_kernel(p->kc);
-    if (!rc) rc = build_twiddles(lr, &p->twc, p->stream);  // pass-2 table (length rows)
+    if (!rc && built_ept != p->k->ept)
+    {
+      // pass 1 runs another variant than the tuned one the tables were built for
+      cudaFree(p->tw);
+      p->tw = nullptr;
+      rc = build_twiddles(lc, p->k->ept, &p->tw, p->stream);
+    }
+    if (!rc) rc = build_twiddles(lr, p->kc->ept, &p->twc, p->stream);  // pass-2 table (length rows)
   }
   if (!rc)
   {

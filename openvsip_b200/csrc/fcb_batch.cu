@@ -326,8 +326,9 @@ int fcb_batch_add_replica(fcb_batch b, const fcb_cf32 *replica, long long n, int
   }
   if (!rc && (e = cudaMalloc(&table, sizeof(float4) * (size_t)(n / 2))) != cudaSuccess)
     rc = set_error(FCB_ERR_NOMEM, "replica table");
-  if (!rc) rc = build_replica_table(l, spec, n, 1, table, b->own_stream);
-  if (!rc && !b->tw[l]) rc = build_twiddles(l, &b->tw[l], b->own_stream);
+  // the batch kernels run 32 samples per thread
+  if (!rc) rc = build_replica_table(l, 32, spec, n, 1, table, b->own_stream);
+  if (!rc && !b->tw[l]) rc = build_twiddles(l, 32, &b->tw[l], b->own_stream);
   if (!rc && (e = cudaStreamSynchronize(b->own_stream)) != cudaSuccess) rc = cuda_error(e, "replica preparation");
   cudaFree(spec);
   cudaFree(tmp);

@@ -98,43 +98,49 @@ int scale_copy(const float2 *in, float2 *out, long long total, float s, cudaStre
 }
 
 // Kernel table of the kChirpconv mode: work rows of 8 .. 65536 samples, the
-// same CTA-size variants as the other modes ([0] 256, [1] 512, [2] 128 threads).
-template <int LOGN, int T>
+// same variants as the other modes ([0] 256, [1] 512, [2] 128 threads with 32
+// samples each, [3] 256 threads with 64 samples for 16384-sample rows).
+template <int LOGN, int T, int EPTW = 32>
 static KernelInfo chirp_info()
 {
-  using S = Sched<LOGN, T>;
+  using S = Sched<LOGN, T, EPTW>;
   KernelInfo k;
-  k.fn = (const void *)&rows_kernel<LOGN, kChirpconv, T>;
+  k.fn = (const void *)&rows_kernel<LOGN, kChirpconv, T, EPTW>;
   k.threads = T;
   k.cluster = S::CS;
   k.rows_per_cta = S::ROWS;
   k.smem = S::SMEM;
   k.tw_bytes = S::tw_bytes();
+  k.ept = EPTW;
   return k;
 }
 
 template <int LOGN>
-static void fill_chirp(KernelInfo (*tab)[3])
+static void fill_chirp(KernelInfo (*tab)[kVariants])
 {
   if constexpr (LOGN >= 3)
   {
     tab[LOGN][0] = chirp_info<LOGN, 256>();
     if constexpr (LOGN >= kMin512) tab[LOGN][1] = chirp_info<LOGN, 512>();
     if constexpr (LOGN >= kMin128 && LOGN <= kMax128) tab[LOGN][2] = chirp_info<LOGN, 128>();
+    if constexpr (LOGN == kWideLog) tab[LOGN][3] = chirp_info<LOGN, 256, 64>();
     fill_chirp<LOGN - 1>(tab);
   }
 }
 
-static KernelInfo g_chirp[kMaxLogN + 1][3];
+static KernelInfo g_chirp[kMaxLogN + 1][kVariants];
 static std::once_flag g_chirp_once;
 
-const KernelInfo *chirp_kernel(int logn, int threads)
+const KernelInfo *chirp_kernel(int logn, const KernelInfo *like)
 {
   std::call_once(g_chirp_once, [] { fill_chirp<kMaxLogN>(g_chirp); });
-  if (logn < 3 || logn > kMaxLogN) return nullptr;
-  const int v = (threads == 512 && logn >= kMin512) ? 1
-              : (threads == 128 && logn >= kMin128 && logn <= kMax128) ? 2 : 0;
-  return &g_chirp[logn][v];
+  if (logn < 3 || logn > kMaxLogN || !like) return nullptr;
+  const int t = like->threads;
+  const int v = (like->ept == 64 && logn == kWideLog) ? 3
+              : (t == 512 && logn >= kMin512) ? 1
+              : (t == 128 && logn >= kMin128 && logn <= kMax128) ? 2 : 0;
+  const KernelInfo *k = &g_chirp[logn][v];
+  return k->ept == like->ept ? k : nullptr;  // the tables it reads are built for like->ept
 }
 
 }  // namespace fcb

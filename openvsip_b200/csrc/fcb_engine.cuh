@@ -10,34 +10,37 @@
 //                               tests/fastconv.cpp:204 (by-value expression)
 //
 // Algorithm (decimation in frequency, "complex pairs"):
-//  * A thread owns 32 complex samples held as 16 complex PAIRS in split form
-//    {re: (a.re, b.re), im: (a.im, b.im)} so that every butterfly, twiddle and
-//    replica multiply runs on Blackwell's packed f32x2 add/mul/fma, two complex
-//    lanes per instruction.
+//  * A thread owns EPT complex samples (32, or 64 in the wide variant) held as
+//    RB = EPT/2 complex PAIRS in split form {re: (a.re, b.re), im: (a.im,
+//    b.im)} so that every butterfly, twiddle and replica multiply runs on
+//    Blackwell's packed f32x2 add/mul/fma, two complex lanes per instruction.
 //  * Stage 1 is a radix-R1 DIF step over the whole row (stride N/R1).  Its first
 //    radix-2 level is done in scalar and places the even-q outputs in lane 0 and
 //    the odd-q outputs in lane 1, so every later operation is lane-parallel with
 //    identical constants in both lanes.  Sub-problem 2q' and 2q'+1 (length
 //    D = N/R1 each) then live side by side in one "slot" (16 bytes).
-//  * Stages 2.. are radix-16 DIF steps inside the sub-problem pairs, in place
-//    in a 16-byte-slot shared-memory array (XOR swizzle against bank conflicts).
-//    A thread reads and writes only its own group's slots inside a stage, so
-//    one barrier per exchange suffices.  Their twiddles are read from a copy
-//    of the tables in shared memory, made once per CTA.
+//  * Stages 2.. are radix-RB DIF steps (16, or 32 in the wide variant) inside
+//    the sub-problem pairs, in place in a 16-byte-slot shared-memory array
+//    (one pad slot per RB slots against bank conflicts).  A thread reads and
+//    writes only its own group's slots inside a stage, so one barrier per
+//    exchange suffices.  Their twiddles are read from a copy of the tables in
+//    shared memory, made once per CTA.  The wide variant needs one stage fewer
+//    at 16384 samples (3 instead of 4: 4 slot exchanges per fused row instead
+//    of 6) at twice the registers per thread.
 //  * Stage-1 twiddles W_N^{nq} for the thread's groups n = t + T*g factor into
-//    W_N^{tq} (loaded once per thread) times W_32^{gq} (a compile-time
-//    constant), because N = 32 T.
+//    W_N^{tq} (loaded once per thread) times W_EPT^{gq} (a compile-time
+//    constant), because N = EPT T.
 //  * After the last forward stage a slot sigma = q'*D + P holds X[k], X[k+1]
-//    with k = 2q' + R1 * digitrev16(P).  The fused path multiplies by a replica
-//    table stored in the order the last stage reads it (the i-th value of
-//    every thread of a row side by side, so each load is coalesced; scaled by
-//    1/N, exact for powers of two) and
-//    runs the exact transpose of the forward stages with conjugate twiddles, so
-//    no reordering pass is ever needed and every row makes one HBM read and one
-//    HBM write.  The standalone FFTs add one reorder exchange.
-//  * A CTA of THREADS threads (256 or 512) holds 32*THREADS samples: several
-//    short rows, one row, or -- for longer rows -- one part of a row, the row
-//    then being spread over a thread-block cluster whose CTAs exchange through
+//    with k = 2q' + R1 * digitrev_RB(P).  The fused path multiplies by a
+//    replica table stored in the order the last stage reads it (the i-th value
+//    of every thread of a row side by side, so each load is coalesced; scaled
+//    by 1/N, exact for powers of two) and runs the exact transpose of the
+//    forward stages with conjugate twiddles, so no reordering pass is ever
+//    needed and every row makes one HBM read and one HBM write.  The
+//    standalone FFTs add one reorder exchange.
+//  * A CTA of THREADS threads holds EPT*THREADS samples: several short rows,
+//    one row, or -- for longer rows -- one part of a row, the row then being
+//    spread over a thread-block cluster whose CTAs exchange through
 //    distributed shared memory in the two exchanges next to stage 1 (stores
 //    forward, loads inverse).  No TMA multicast is used anywhere.
 #pragma once
@@ -55,29 +58,31 @@ constexpr int kMaxLogN = 16;
 
 // ---------------------------------------------------------------------------
 // Schedule of a length-2^LOGN row transform on CTAs of THREADS threads.
-template <int LOGN, int THREADS>
+template <int LOGN, int THREADS, int EPTW = 32>
 struct Sched
 {
   static constexpr int T = THREADS;
   static constexpr int N = 1 << LOGN;
-  static constexpr int NS = (LOGN <= 5) ? 1 : 1 + (LOGN - 5 + 3) / 4;  // stages
-  static constexpr int LOGR1 = LOGN - 4 * (NS - 1);
+  static constexpr int RB = EPTW / 2;               // radix of the later stages (pairs per thread)
+  static constexpr int LRB = EPTW == 64 ? 5 : 4;
+  static constexpr int NS = (LOGN <= LRB + 1) ? 1 : 1 + (LOGN - (LRB + 1) + LRB - 1) / LRB;  // stages
+  static constexpr int LOGR1 = LOGN - LRB * (NS - 1);
   static constexpr int R1 = 1 << LOGR1;
   static constexpr int H1 = R1 / 2;                 // pairs per stage-1 group
   static constexpr int D = N / R1;                  // sub-problem length
-  static constexpr int EPT = N < 32 ? N : 32;       // samples per thread
+  static constexpr int EPT = N < EPTW ? N : EPTW;   // samples per thread
   static constexpr int CPT = EPT / 2;               // pairs per thread
   static constexpr int TPR = N / EPT;               // threads per row (cluster-wide)
   static constexpr int G1 = EPT / R1;               // stage-1 groups per thread
-  static constexpr int SPC = T * 16;                // slots per CTA for rows of >= 32 samples
+  static constexpr int SPC = T * RB;                // slots per CTA for rows of >= EPTW samples
   static constexpr int HALF = N / 2;                // slots per row
   static constexpr int CS = HALF > SPC ? HALF / SPC : 1;  // CTAs per cluster
   static constexpr int TPRL = TPR / CS;             // threads per row per CTA
   static constexpr int ROWS = CS > 1 ? 1 : T / TPR; // rows per CTA
   static constexpr int SLOTS = CS > 1 ? SPC : ROWS * HALF;  // slots per CTA
   // stage s (2..NS): block length and stride in slots
-  __host__ __device__ static constexpr int L(int s) { return D >> (4 * (s - 2)); }
-  __host__ __device__ static constexpr int S(int s) { return L(s) / 16; }
+  __host__ __device__ static constexpr int L(int s) { return D >> (LRB * (s - 2)); }
+  __host__ __device__ static constexpr int S(int s) { return L(s) / RB; }
   // Twiddle tables in global memory: stage 1 as HALF float4 entries, then
   // stages 2..NS as float2 entries at tw2_off(s) (float2 units, counted after
   // the float4 part).  Stages 2..NS-1 (the ones with twiddles) are copied to
@@ -90,7 +95,7 @@ struct Sched
   }
   __host__ __device__ static constexpr int tw_bytes() { return HALF * 16 + tw2_off(NS + 1) * 8; }
   static constexpr int TWS = NS >= 3 ? tw2_off(NS) : 0;   // float2 entries kept in shared memory
-  static constexpr int SMEM = (SLOTS + SLOTS / 16) * 16 + TWS * 8;  // padded slots, then twiddles
+  static constexpr int SMEM = (SLOTS + SLOTS / RB) * 16 + TWS * 8;  // padded slots, then twiddles
 };
 
 
@@ -141,6 +146,19 @@ __host__ __device__ constexpr float c32h(int k) { return k <= 8 ? cq32(k) : -cq3
 __host__ __device__ constexpr float s32h(int k) { return k <= 8 ? cq32(8 - k) : cq32(k - 8); }
 __host__ __device__ constexpr float c32(int k) { return k < 16 ? c32h(k) : -c32h(k - 16); }
 __host__ __device__ constexpr float s32(int k) { return k < 16 ? s32h(k) : -s32h(k - 16); }
+
+__host__ __device__ constexpr float cq64(int k)
+{
+  return k == 0 ? 1.0f : k == 1 ? 0.9951847195625305f : k == 2 ? 0.9807852506637573f : k == 3 ? 0.9569403529167175f
+       : k == 4 ? 0.9238795042037964f : k == 5 ? 0.8819212913513184f : k == 6 ? 0.8314695954322815f
+       : k == 7 ? 0.7730104327201843f : k == 8 ? 0.7071067690849304f : k == 9 ? 0.6343932747840881f
+       : k == 10 ? 0.5555702447891235f : k == 11 ? 0.4713967442512512f : k == 12 ? 0.3826834261417389f
+       : k == 13 ? 0.290284663438797f : k == 14 ? 0.19509032368659973f : k == 15 ? 0.0980171412229538f : 0.0f;
+}
+__host__ __device__ constexpr float c64h(int k) { return k <= 16 ? cq64(k) : -cq64(32 - k); }
+__host__ __device__ constexpr float s64h(int k) { return k <= 16 ? cq64(16 - k) : cq64(k - 16); }
+__host__ __device__ constexpr float c64(int k) { return k < 32 ? c64h(k) : -c64h(k - 32); }
+__host__ __device__ constexpr float s64(int k) { return k < 32 ? s64h(k) : -s64h(k - 32); }
 
 // Multiply a pair by the constant W_32^K = exp(SIGN * 2 pi i K / 32), 0 <= K < 16.
 template <int K, int SIGN>
@@ -214,21 +232,22 @@ __host__ __device__ constexpr int bitrev(int i, int bits)
 }
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
-// Reverse the 4-bit digits of p (ndig digits).
-__host__ __device__ __forceinline__ int digitrev16(int p, int ndig)
+// Reverse the lb-bit digits of p (ndig digits; lb = log2 of the later-stage radix).
+__host__ __device__ __forceinline__ int digitrev16(int p, int ndig, int lb = 4)
 {
   int r = 0;
-  for (int d = 0; d < ndig; ++d) { r = (r << 4) | (p & 15); p >>= 4; }
+  for (int d = 0; d < ndig; ++d) { r = (r << lb) | (p & ((1 << lb) - 1)); p >>= lb; }
   return r;
 }
 
 // Physical position of slot i in shared memory: one padding slot after every
-// 16 slots.  Every exchange pattern of the kernel (consecutive slots across
-// threads, slots 16 apart across threads for the last stage) then falls on
-// distinct 16-byte banks, and for the stride patterns of a stage the physical
-// address stays linear in the element index, so the compiler folds the
-// per-element offsets into the load/store instructions.
-__device__ __forceinline__ int swz(int i) { return i + (i >> 4); }
+// 2^lb slots (lb = log2 of the later-stage radix, 4 or 5).  Every exchange
+// pattern of the kernel (consecutive slots across threads, slots 2^lb apart
+// across threads for the last stage) then falls on distinct 16-byte banks,
+// and for the stride patterns of a stage the physical address stays linear in
+// the element index, so the compiler folds the per-element offsets into the
+// load/store instructions.
+__device__ __forceinline__ int swz(int i, int lb = 4) { return i + (i >> lb); }
 
 // Loads that stay where they are written: volatile asm is not moved across
 // other volatile asm or memory operations, so twiddle and replica loads are
@@ -296,6 +315,16 @@ __device__ __forceinline__ cpair cp_mul4c(cpair x, float4 w)
 {
   return cp_mul<true>(x, make_float2(w.x, w.y), make_float2(w.z, w.w));
 }
+// Per-lane constant rotation by W_64^{k0}, W_64^{k1} (k in units of 2 pi / 64).
+template <int SIGN>
+__device__ __forceinline__ cpair cp_rot2w(cpair x, int k0, int k1)
+{
+  if (k0 == 0 && k1 == 0) return x;
+  const float2 c = make_float2(c64(k0), c64(k1));
+  const float2 s = make_float2(SIGN * s64(k0), SIGN * s64(k1));
+  return {f2fma(x.im, f2neg(s), f2mul(x.re, c)), f2fma(x.re, s, f2mul(x.im, c))};
+}
+
 // Per-lane constant rotation: lane 0 by W_32^{k0}, lane 1 by W_32^{k1}, with
 // W_32 = exp(SIGN 2 pi i / 32).  k0, k1 are compile-time constants after
 // unrolling, so the cos/sin pairs fold to immediates.
@@ -398,15 +427,18 @@ __device__ __forceinline__ void group_sync(int t)
 // while consecutive tiles have the same length).  The caller guarantees that
 // no thread of the CTA (or of the CS CTAs) still reads the slot array of a
 // previous tile.
-template <int LOGN, int MODE, int THREADS>
+template <int LOGN, int MODE, int THREADS, int EPTW = 32>
 __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int rank, int rank_base, bool copy_tw)
 {
-  using S = Sched<LOGN, THREADS>;
+  using S = Sched<LOGN, THREADS, EPTW>;
+  constexpr int RB = S::RB, LRB = S::LRB;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
   constexpr bool CHIRP = MODE == kChirpconv;
   constexpr int MD = CHIRP ? kFastconv : MODE;    // the transform structure
   constexpr int LH1 = ilog2(S::H1);
   constexpr bool CL = S::CS > 1;
+  // stage 2 reads its block of D slots from its own CTA only
+  static_assert(!CL || S::D <= S::SPC, "a stage-2 block must lie within one CTA of the cluster");
   extern __shared__ float4 smem[];
   const float2 *tw2 = reinterpret_cast<const float2 *>(a.tw + S::HALF);
 
@@ -426,8 +458,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     for (int r = 0; r < S::CS; ++r) peer[r] = cluster_addr(own, rank_base + r);
   }
   const uint32_t slot_base = smem_addr(smem);
-  const uint32_t tw_base = slot_base + 16u * (S::SLOTS + S::SLOTS / 16);  // later-stage twiddles
-  auto slot_addr = [&](int local) { return slot_base + 16u * (uint32_t)swz(local); };
+  const uint32_t tw_base = slot_base + 16u * (S::SLOTS + S::SLOTS / RB);  // later-stage twiddles
+  auto swz_ = [&](int i) { return swz(i, LRB); };
+  auto slot_addr = [&](int local) { return slot_base + 16u * (uint32_t)swz_(local); };
 
   // copy the twiddle tables of stages 2..NS-1 to shared memory (read before
   // the first barrier below, used after it)
@@ -531,9 +564,9 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         {
           const int qp = bitrev(i, LH1);
           cpair v = (SIGN < 0) ? cp_mul4(cg1[i], tw1[i]) : cp_mul4c(cg1[i], tw1[i]);
-          v = cp_rot2<SIGN>(v, (g * 2 * qp) & 31, (g * (2 * qp + 1)) & 31);
+          v = (EPTW == 64) ? cp_rot2w<SIGN>(v, (g * 2 * qp) & 63, (g * (2 * qp + 1)) & 63) : cp_rot2<SIGN>(v, (g * 2 * qp) & 31, (g * (2 * qp + 1)) & 31);
           const int sigma = qp * S::D + n;
-          st_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)), cp_to4(v));
+          st_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz_(SlotMap<S>::local(sigma, rho)), cp_to4(v));
         }
       }
     }
@@ -554,7 +587,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     const int base = B * Lg + n;
     const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
 #pragma unroll
-    for (int r = 0; r < 16; ++r)
+    for (int r = 0; r < RB; ++r)
       c[r] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * r, rho))));
     float4 ra[4];  // replica entries, four at a time
     if constexpr (MD == kFastconv && s == S::NS)
@@ -562,12 +595,12 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 #pragma unroll
       for (int i = 0; i < 4; ++i) ra[i] = ldv4(rp + i * S::TPR + tr);
     }
-    DifNet<16, SIGN>::run(c);
+    DifNet<RB, SIGN>::run(c);
     if constexpr (St > 1)
     {
       // twiddles in batches of four: fewer live registers (no spills)
 #pragma unroll
-      for (int b = 0; b < 16; b += 4)
+      for (int b = 0; b < RB; b += 4)
       {
         float2 w[4];
 #pragma unroll
@@ -576,7 +609,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
-          const int q = b + j, i = bitrev(q, 4);
+          const int q = b + j, i = bitrev(q, LRB);
           if (q != 0)
             c[i] = (SIGN < 0) ? cp_mul<false>(c[i], f2dup(w[j].x), f2dup(w[j].y))
                               : cp_mul<true>(c[i], f2dup(w[j].x), f2dup(w[j].y));
@@ -586,7 +619,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     if constexpr (MD == kFastconv && s == S::NS)
     {
 #pragma unroll
-      for (int b = 0; b < 16; b += 4)
+      for (int b = 0; b < RB; b += 4)
       {
         if (b > 0)
         {
@@ -600,8 +633,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     if constexpr (s < S::NS)
     {
 #pragma unroll
-      for (int i = 0; i < 16; ++i)
-        st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, 4), rho)), cp_to4(c[i]));
+      for (int i = 0; i < RB; ++i)
+        st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, LRB), rho)), cp_to4(c[i]));
       group_sync<St, THREADS>(t);  // stage s+1 reads only this block of Lg slots
     }
   };
@@ -613,8 +646,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   {
     // ---------------- reorder to natural frequency order and store ----------------
     // c[] holds the last stage's outputs (never written back).  Pair slot
-    // sigma = q'*D + P holds X[k], X[k+1] with k = 2q' + R1 * digitrev16(P), so it
-    // moves to natural pair index m = q' + (R1/2) * digitrev16(P).
+    // sigma = q'*D + P holds X[k], X[k+1] with k = 2q' + R1 * digitrev_RB(P), so it
+    // moves to natural pair index m = q' + (R1/2) * digitrev_RB(P).
     int dst[S::CPT];
     if constexpr (S::NS == 1)
     {
@@ -626,10 +659,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       constexpr int Lg = S::L(S::NS), St = S::S(S::NS);
       const int B = tr / St, n = tr % St;
 #pragma unroll
-      for (int i = 0; i < 16; ++i)
+      for (int i = 0; i < RB; ++i)
       {
-        const int sigma = B * Lg + n + St * bitrev(i, 4);
-        dst[i] = sigma / S::D + S::H1 * digitrev16(sigma % S::D, S::NS - 1);
+        const int sigma = B * Lg + n + St * bitrev(i, LRB);
+        dst[i] = sigma / S::D + S::H1 * digitrev16(sigma % S::D, S::NS - 1, LRB);
       }
     }
     if constexpr (CL) cluster_sync(); else __syncthreads();
@@ -637,7 +670,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     for (int i = 0; i < S::CPT; ++i)
     {
       const int m = dst[i];
-      st_slot<CL>(peer[SlotMap<S>::owner(m)] + 16u * swz(SlotMap<S>::local(m, rho)), cp_to4(c[i]));
+      st_slot<CL>(peer[SlotMap<S>::owner(m)] + 16u * swz_(SlotMap<S>::local(m, rho)), cp_to4(c[i]));
     }
     if constexpr (CL) cluster_sync(); else __syncthreads();
     // natural-order read of this CTA's part of the row, scale, store.
@@ -715,22 +748,22 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       constexpr int Lg = S::L(s), St = S::S(s);
       const int B = tr / St, n = tr % St;
       const int base = B * Lg + n;
-      cpair z[16];
+      cpair z[RB];
       if constexpr (s < S::NS)
       {
 #pragma unroll
-        for (int q = 0; q < 16; ++q)
+        for (int q = 0; q < RB; ++q)
           z[q] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * q, rho))));
       }
       else
       {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) z[bitrev(i, 4)] = c[i];
+        for (int i = 0; i < RB; ++i) z[bitrev(i, LRB)] = c[i];
       }
       if constexpr (St > 1)
       {
 #pragma unroll
-        for (int b = 0; b < 16; b += 4)
+        for (int b = 0; b < RB; b += 4)
         {
           float2 w[4];
 #pragma unroll
@@ -741,10 +774,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
             if (b + j > 0) z[b + j] = cp_mul<true>(z[b + j], f2dup(w[j].x), f2dup(w[j].y));
         }
       }
-      DifNet<16, +1>::run(z);  // z[i] = y[bitrev(i)]
+      DifNet<RB, +1>::run(z);  // z[i] = y[bitrev(i)]
 #pragma unroll
-      for (int i = 0; i < 16; ++i)
-        st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, 4), rho)), cp_to4(z[i]));
+      for (int i = 0; i < RB; ++i)
+        st_slot<false>(slot_addr(SlotMap<S>::local(base + St * bitrev(i, LRB), rho)), cp_to4(z[i]));
       if constexpr (s > 2) group_sync<S::S(s - 1), THREADS>(t);  // stage s-1 reads blocks of L(s-1)
     };
     if constexpr (S::NS >= 4) stage_inv(ic<4>{});
@@ -774,7 +807,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         for (int qp = 0; qp < S::H1; ++qp)
         {
           const int sigma = qp * S::D + tr + S::TPR * g;
-          v[g * S::H1 + qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz(SlotMap<S>::local(sigma, rho)));
+          v[g * S::H1 + qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz_(SlotMap<S>::local(sigma, rho)));
         }
     }
 #pragma unroll
@@ -786,8 +819,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       {
 #pragma unroll
         for (int qp = 0; qp < S::H1; ++qp)
-          z[qp] = cp_rot2<+1>(cp_mul4c(cp_from4(v[g * S::H1 + qp]), tw1[qp]), (g * 2 * qp) & 31,
-                              (g * (2 * qp + 1)) & 31);
+          z[qp] = (EPTW == 64) ? cp_rot2w<+1>(cp_mul4c(cp_from4(v[g * S::H1 + qp]), tw1[qp]), (g * 2 * qp) & 63,
+                                              (g * (2 * qp + 1)) & 63)
+                               : cp_rot2<+1>(cp_mul4c(cp_from4(v[g * S::H1 + qp]), tw1[qp]), (g * 2 * qp) & 31,
+                                             (g * (2 * qp + 1)) & 31);
       }
       else
       {
@@ -830,14 +865,14 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 }
 
 // Standalone launch: one tile per CTA, or per cluster of CS CTAs.
-template <int LOGN, int MODE, int THREADS>
-__global__ void __launch_bounds__(THREADS, 512 / THREADS) rows_kernel(RowArgs a)
+template <int LOGN, int MODE, int THREADS, int EPTW = 32>
+__global__ void __launch_bounds__(THREADS, (EPTW == 32 ? 512 : 256) / THREADS) rows_kernel(RowArgs a)
 {
-  using S = Sched<LOGN, THREADS>;
+  using S = Sched<LOGN, THREADS, EPTW>;
   if constexpr (S::CS > 1)
-    row_tile<LOGN, MODE, THREADS>(a, blockIdx.x / S::CS, (int)cg::this_cluster().block_rank(), 0, true);
+    row_tile<LOGN, MODE, THREADS, EPTW>(a, blockIdx.x / S::CS, (int)cg::this_cluster().block_rank(), 0, true);
   else
-    row_tile<LOGN, MODE, THREADS>(a, blockIdx.x, 0, 0, true);
+    row_tile<LOGN, MODE, THREADS, EPTW>(a, blockIdx.x, 0, 0, true);
 }
 
 }  // namespace fcb

@@ -11,9 +11,10 @@ struct RowArgs;
 struct SchedRT
 {
   int logn, n, ns, r1, d, half;
+  int ept, rb, lrb;    // samples per thread, later-stage radix and its log2
   long long tw2_size;  // float2 entries of the stage >= 2 twiddle tables
 };
-SchedRT sched_rt(int logn);
+SchedRT sched_rt(int logn, int ept = 32);
 
 struct KernelInfo
 {
@@ -23,24 +24,30 @@ struct KernelInfo
   int rows_per_cta = 1;  // rows per CTA when cluster == 1
   int smem = 0;          // dynamic shared memory per CTA, bytes
   long long tw_bytes = 0; // twiddle table size
+  int ept = 32;          // samples per thread (the tables depend on it)
   long long resident_tiles = 0;  // CTAs (or clusters) resident at once, set by prepare_kernel
 };
 
 constexpr int kMin512 = 12;  // 512-thread variants exist for rows of 4096 samples and more
-constexpr int kMin128 = 8, kMax128 = 14;  // 128-thread variants: rows of 256 .. 16384 samples
+constexpr int kMin128 = 8, kMax128 = 13;  // 128-thread variants: rows of 256 .. 8192 samples
+constexpr int kWideLog = 14;  // the wide variant (256 threads x 64 samples): rows of 16384 samples
+// Variant ids: [0] 256, [1] 512, [2] 128 threads with 32 samples each, [3] the
+// wide one.  Its public tuning value is -256.
+constexpr int kVariants = 4;
 
 const KernelInfo *kernel_info(int logn, int mode);
 // Fused kernel with element-wise multipliers (kChirpconv, fcb_bluestein.cu)
-// for work rows of 2^logn samples, CTA size as close to `threads` as exists.
-const KernelInfo *chirp_kernel(int logn, int threads);
+// for work rows of 2^logn samples, in the same variant as `like` (whose
+// tables it reads).
+const KernelInfo *chirp_kernel(int logn, const KernelInfo *like);
 int set_variant(int logn, int mode, int threads);
 const KernelInfo *kernel_variant(int logn, int mode, int threads);
 int get_variant(int logn, int mode);
 int prepare_kernel(const KernelInfo *k);
 int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaStream_t st);
 
-int build_twiddles(int logn, float4 **out, cudaStream_t st);
-int build_replica_table(int logn, const float2 *spec_dev, long long spec_rs, long long rows,
+int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st);
+int build_replica_table(int logn, int ept, const float2 *spec_dev, long long spec_rs, long long rows,
                         float4 *rep_dev, cudaStream_t st);
 int replica_spectrum_dev(const float2 *rep_dev, long long n, int matched, float2 *spec_dev,
                          cudaStream_t st);

@@ -55,3 +55,22 @@ def oracle():
 
 def crandn(rng, shape, scale=1.0):
     return ((rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * scale).astype(np.complex64)
+
+
+class pinned_variant:
+    """Temporarily select a kernel variant (fcb_tune_set) for length n and kind
+    (0 forward, 1 inverse, 2 fused), restoring the previous one on exit."""
+
+    def __init__(self, n, kind, threads):
+        self.n, self.kind, self.threads = n, kind, threads
+
+    def __enter__(self):
+        from openvsip_b200 import _lib
+        self.lib = _lib.lib()
+        self.saved = self.lib.fcb_tune_get(self.n, self.kind)
+        _lib.check(self.lib.fcb_tune_set(self.n, self.kind, self.threads))
+        return self
+
+    def __exit__(self, *exc):
+        from openvsip_b200 import _lib
+        _lib.check(self.lib.fcb_tune_set(self.n, self.kind, self.saved))

@@ -11,7 +11,8 @@ def test_variants_per_length():
     assert autotune.variants(64) == (256,)
     assert autotune.variants(256) == (128, 256)
     assert autotune.variants(4096) == (128, 256, 512)
-    assert autotune.variants(16384) == (128, 256, 512)
+    assert autotune.variants(8192) == (128, 256, 512)
+    assert autotune.variants(16384) == (256, 512, -256)
     assert autotune.variants(32768) == (256, 512)
 
 
@@ -35,5 +36,5 @@ def test_tune_installs_choice_and_cache_round_trip(tmp_path, monkeypatch):
     autotune.load(path)
     assert lib.fcb_tune_get(1024, autotune.KINDS["fastconv"]) == res["fastconv:1024"]["threads"]
     # leave the library defaults for the tests that follow
-    for n, t in ((1024, 128), (16384, 512)):
+    for n, t in ((1024, 128), (16384, -256)):
         _lib.check(lib.fcb_tune_set(n, autotune.KINDS["fastconv"], t))

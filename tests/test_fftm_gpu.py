@@ -88,3 +88,30 @@ def test_fftm_accuracy_vs_fp32_cpu_fft(oracle, n):
     assert cpu.dtype == np.complex64
     gpu = Fftm(16, n, fft_fwd, 1.0)(x)
     assert oracle.rel_l2(gpu, ref) <= 2 * oracle.rel_l2(cpu, ref) + 1e-9
+
+
+@pytest.mark.parametrize("threads", [-256, 512, 256])
+def test_every_variant_at_16384(oracle, threads):
+    # all kernel variants of 16384-sample rows, forward, inverse and fused
+    # (-256: 256 threads x 64 samples, 3 stages; the others 32 samples, 4
+    # stages; 256: a cluster of two CTAs)
+    from openvsip_b200 import Fastconv, _lib
+    lib = _lib.lib()
+    n, rows = 16384, 24
+    saved = [lib.fcb_tune_get(n, k) for k in range(3)]
+    try:
+        for k in range(3):
+            _lib.check(lib.fcb_tune_set(n, k, threads))
+        rng = np.random.default_rng(700 + threads)
+        x = crandn(rng, (rows, n))
+        rep = crandn(rng, (n,))
+        f = Fftm(rows, n, fft_fwd, 1.0)
+        assert f.info()["threads"] == abs(threads)
+        assert oracle.rel_l2(f(x), oracle.fft_rows(x, -1)) <= RTOL
+        assert oracle.rel_l2(Fftm(rows, n, fft_inv, 1.0 / n)(x), oracle.fft_rows(x, +1, 1.0 / n)) <= RTOL
+        w = crandn(rng, (rows, n))
+        assert oracle.rel_l2(Fastconv(rep, rows)(x), oracle.fastconv(x, rep)) <= RTOL
+        assert oracle.rel_l2(Fastconv(w, rows)(x), oracle.fastconv(x, w)) <= RTOL
+    finally:
+        for k in range(3):
+            _lib.check(lib.fcb_tune_set(n, k, saved[k]))
