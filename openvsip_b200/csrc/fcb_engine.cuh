@@ -96,6 +96,12 @@ struct Sched
   __host__ __device__ static constexpr int tw_bytes() { return HALF * 16 + tw2_off(NS + 1) * 8; }
   static constexpr int TWS = NS >= 3 ? tw2_off(NS) : 0;   // float2 entries kept in shared memory
   static constexpr int SMEM = (SLOTS + SLOTS / RB) * 16 + TWS * 8;  // padded slots, then twiddles
+  // CTAs resident per SM (the register file holds 512 threads of 32 samples or
+  // 256 of 64), the launch bound's minimum
+  static constexpr int MINB = (EPTW == 32 ? 512 : 256) / THREADS;
+  // With one CTA per SM its two halves run out of phase through the
+  // sub-problem stages (see row_tile)
+  static constexpr bool STAGGER = MINB == 1 && NS >= 3;
 };
 
 
@@ -412,12 +418,23 @@ __device__ __forceinline__ void cluster_sync()
 template <int NT, int THREADS>
 __device__ __forceinline__ void group_sync(int t)
 {
+  static_assert(NT <= 32 || NT >= THREADS || THREADS / NT <= 13, "named barriers 14 and 15 are the stagger barriers");
   if constexpr (NT <= 32)
     __syncwarp();
   else if constexpr (NT >= THREADS)
     __syncthreads();
   else
     asm volatile("bar.sync %0, %1;" :: "r"(1 + t / NT), "r"(NT) : "memory");
+}
+
+// Stagger barriers: the first half of a CTA arrives, the second half waits.
+__device__ __forceinline__ void half_arrive(int id, int threads)
+{
+  asm volatile("bar.arrive %0, %1;" :: "r"(id), "r"(threads) : "memory");
+}
+__device__ __forceinline__ void half_wait(int id, int threads)
+{
+  asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(threads) : "memory");
 }
 
 // One tile of a row transform on this CTA: the ROWS rows of `tile` when a row
@@ -439,6 +456,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   constexpr bool CL = S::CS > 1;
   // stage 2 reads its block of D slots from its own CTA only
   static_assert(!CL || S::D <= S::SPC, "a stage-2 block must lie within one CTA of the cluster");
+  static_assert(!S::STAGGER || S::S(2) <= THREADS / 2, "a stage-2 block must lie within one half of the CTA");
   extern __shared__ float4 smem[];
   const float2 *tw2 = reinterpret_cast<const float2 *>(a.tw + S::HALF);
 
@@ -586,9 +604,20 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     const int B = tr / St, n = tr % St;
     const int base = B * Lg + n;
     const float4 *rp = a.rep + (active ? row : 0) * a.rep_rs;  // inactive rows read row 0
+    // Stagger (one CTA per SM, whose warps would otherwise all be reading or
+    // writing slots at the same time and then all computing): the second half
+    // of the CTA starts stage 2 once the first half has issued its slot reads.
+    // A block of stage 2 or later belongs to at most half of the CTA, and the
+    // halves meet again only at the barrier before the inverse stage 1, so
+    // from here on one half's shared-memory traffic overlaps the other half's
+    // arithmetic.
+    if constexpr (s == 2 && S::STAGGER)
+      if (t >= THREADS / 2) half_wait(15, THREADS);
 #pragma unroll
     for (int r = 0; r < RB; ++r)
       c[r] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * r, rho))));
+    if constexpr (s == 2 && S::STAGGER)
+      if (t < THREADS / 2) half_arrive(15, THREADS);
     float4 ra[4];  // replica entries, four at a time
     if constexpr (MD == kFastconv && s == S::NS)
     {
@@ -801,6 +830,10 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     float4 v[S::CPT];
     if constexpr (S::NS > 1)
     {
+      // the same stagger for the inverse stage 1: the second half reads its
+      // slots once the first half has issued its reads
+      if constexpr (S::STAGGER)
+        if (t >= THREADS / 2) half_wait(14, THREADS);
 #pragma unroll
       for (int g = 0; g < S::G1; ++g)
 #pragma unroll
@@ -809,6 +842,8 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
           const int sigma = qp * S::D + tr + S::TPR * g;
           v[g * S::H1 + qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz_(SlotMap<S>::local(sigma, rho)));
         }
+      if constexpr (S::STAGGER)
+        if (t < THREADS / 2) half_arrive(14, THREADS);
     }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
@@ -866,7 +901,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
 
 // Standalone launch: one tile per CTA, or per cluster of CS CTAs.
 template <int LOGN, int MODE, int THREADS, int EPTW = 32>
-__global__ void __launch_bounds__(THREADS, (EPTW == 32 ? 512 : 256) / THREADS) rows_kernel(RowArgs a)
+__global__ void __launch_bounds__(THREADS, (Sched<LOGN, THREADS, EPTW>::MINB)) rows_kernel(RowArgs a)
 {
   using S = Sched<LOGN, THREADS, EPTW>;
   if constexpr (S::CS > 1)
