@@ -427,14 +427,17 @@ __device__ __forceinline__ void group_sync(int t)
     asm volatile("bar.sync %0, %1;" :: "r"(1 + t / NT), "r"(NT) : "memory");
 }
 
-// Stagger barriers: the first half of a CTA arrives, the second half waits.
-__device__ __forceinline__ void half_arrive(int id, int threads)
+// Stagger barriers (IDs as immediates): the first half of a CTA arrives, the
+// second half waits; THREADS threads in all.
+template <int ID, int THREADS>
+__device__ __forceinline__ void half_arrive()
 {
-  asm volatile("bar.arrive %0, %1;" :: "r"(id), "r"(threads) : "memory");
+  asm volatile("bar.arrive %0, %1;" :: "n"(ID), "n"(THREADS) : "memory");
 }
-__device__ __forceinline__ void half_wait(int id, int threads)
+template <int ID, int THREADS>
+__device__ __forceinline__ void half_wait()
 {
-  asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(threads) : "memory");
+  asm volatile("bar.sync %0, %1;" :: "n"(ID), "n"(THREADS) : "memory");
 }
 
 // One tile of a row transform on this CTA: the ROWS rows of `tile` when a row
@@ -612,12 +615,12 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     // from here on one half's shared-memory traffic overlaps the other half's
     // arithmetic.
     if constexpr (s == 2 && S::STAGGER)
-      if (t >= THREADS / 2) half_wait(15, THREADS);
+      if (t >= THREADS / 2) half_wait<15, THREADS>();
 #pragma unroll
     for (int r = 0; r < RB; ++r)
       c[r] = cp_from4(ld_slot<false>(slot_addr(SlotMap<S>::local(base + St * r, rho))));
     if constexpr (s == 2 && S::STAGGER)
-      if (t < THREADS / 2) half_arrive(15, THREADS);
+      if (t < THREADS / 2) half_arrive<15, THREADS>();
     float4 ra[4];  // replica entries, four at a time
     if constexpr (MD == kFastconv && s == S::NS)
     {
@@ -833,7 +836,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
       // the same stagger for the inverse stage 1: the second half reads its
       // slots once the first half has issued its reads
       if constexpr (S::STAGGER)
-        if (t >= THREADS / 2) half_wait(14, THREADS);
+        if (t >= THREADS / 2) half_wait<14, THREADS>();
 #pragma unroll
       for (int g = 0; g < S::G1; ++g)
 #pragma unroll
@@ -843,7 +846,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
           v[g * S::H1 + qp] = ld_slot<CL>(peer[SlotMap<S>::owner(sigma)] + 16u * swz_(SlotMap<S>::local(sigma, rho)));
         }
       if constexpr (S::STAGGER)
-        if (t < THREADS / 2) half_arrive(14, THREADS);
+        if (t < THREADS / 2) half_arrive<14, THREADS>();
     }
 #pragma unroll
     for (int g = 0; g < S::G1; ++g)
