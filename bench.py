@@ -577,7 +577,7 @@ def main():
             "fftw_standin": standin,
             "e2e": {"value": e2e_value, "unit": "complex samples/s", "h2d_bytes_per_step": x_host.nbytes,
                     "d2h_bytes_per_step": x_host.nbytes, "steps": e2e_steps,
-                    "how": "Fastconv(host pinned in, host pinned out): chunked H2D/kernel/D2H on 2 streams"},
+                    "how": "Fastconv(host pinned in, host pinned out): chunked H2D / kernel / D2H on three streams"},
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }
