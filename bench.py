@@ -506,28 +506,36 @@ def main():
     ref = np.fft.ifft(np.fft.fft(xs, axis=1) * rep.astype(np.complex128), axis=1)
     rel = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
 
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
+    # throughput: K back-to-back launches between two events
     with ClockSampler(local) as clk:
         t_start.record(stream)
         for i in range(args.steps):
-            starts[i].record(stream)
             fc(xin[i % 2], yout)
-            ends[i].record(stream)
         t_end.record(stream)
         torch.cuda.synchronize()
     barrier()
-    total_ms = t_start.elapsed_time(t_end)
+    local_ms = t_start.elapsed_time(t_end)
+    total_ms = shard.max_over_ranks(local_ms)  # max over ranks (NCCL all-reduce of one scalar)
+
+    # per-launch latency (p50 / p99): a second pass with one event pair around each launch,
+    # outside the throughput region so that its event records do not count there
+    lat_steps = min(args.steps, 200)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(lat_steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(lat_steps)]
+    for i in range(lat_steps):
+        starts[i].record(stream)
+        fc(xin[i % 2], yout)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = shard.max_over_ranks(total_ms)  # max over ranks (NCCL all-reduce of one scalar)
 
     samples_step = pulses * nsamp
     value = samples_step * args.steps * world / (total_ms / 1e3)
-    launch_ms = sum(step_ms) / len(step_ms)
+    launch_ms = local_ms / args.steps  # average launch duration over the timed region
     alg_bytes = 16.0 * samples_step + 8.0 * nsamp
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     peak, peak_src = measured_peak()
@@ -567,7 +575,8 @@ def main():
                                   "smem_bytes": info["smem_bytes"],
                                   "variant": int(ov.lib().fcb_tune_get(nsamp, 2))}},
             "latency_ms": {"p50": sorted_ms[len(sorted_ms) // 2],
-                           "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))]},
+                           "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))],
+                           "launches": lat_steps},
             "rel_l2_vs_fp64": rel,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic() if default_shape else None,
