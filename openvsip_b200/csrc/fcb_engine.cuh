@@ -379,6 +379,12 @@ __device__ __forceinline__ void prefetch_l2(const void *p)
   asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
 }
 
+// Bulk prefetch into L2 of `bytes` bytes (16-byte aligned start, a multiple of 16 bytes).
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, uint32_t bytes)
+{
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" :: "l"(p), "r"(bytes) : "memory");
+}
+
 // kChirpconv is the fused fast convolution with element-wise multipliers and
 // zero padding on the way in and truncation on the way out (Bluestein rows).
 enum Mode { kFwd = 0, kInv = 1, kFastconv = 2, kChirpconv = 3 };
@@ -533,20 +539,32 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
     // With this tile's loads in flight, prefetch into L2 the input of the tile
     // `ahead` tiles later (about half a resident wave), so that it streams in
     // from HBM while this tile computes.  Straight-line code (a few lines per
-    // thread) placed here measured faster than a loop at the kernel start.
+    // thread) placed here measured faster than a loop at the kernel start.  A
+    // CTA of a cluster of four or more prefetches its part of the row with one
+    // bulk prefetch when that part is 16-byte aligned (measured 6 % faster at
+    // 65536 samples; at 32768 samples and for single-CTA rows the per-line
+    // prefetch measured as fast or faster).
     {
       constexpr int LPR = S::N >= 16 ? S::N / 16 : 1;          // 128-byte lines per row
       constexpr int LINES = S::ROWS * LPR / S::CS;             // lines of this CTA's part
       constexpr int PER = (LINES + THREADS - 1) / THREADS;
       const long long row0 = (tile + a.ahead) * S::ROWS;
-#pragma unroll
-      for (int k = 0; k < PER; ++k)
+      const char *part = reinterpret_cast<const char *>(a.in + row0 * a.in_rs) + rank * (8LL * S::N / S::CS);
+      if (S::CS >= 4 && !CHIRP && (reinterpret_cast<uintptr_t>(part) & 15) == 0)
       {
-        const int i = t + THREADS * k;
-        const int li = rank * LINES + i;
-        const long long r = row0 + li / LPR;
-        if (a.ahead > 0 && i < LINES && r < a.rows && (!CHIRP || (li % LPR) * 16 < a.n_in))
-          prefetch_l2(a.in + r * a.in_rs + (li % LPR) * 16);
+        if (a.ahead > 0 && t == 0 && row0 < a.rows) prefetch_l2_bulk(part, (uint32_t)(8LL * S::N / S::CS));
+      }
+      else
+      {
+#pragma unroll
+        for (int k = 0; k < PER; ++k)
+        {
+          const int i = t + THREADS * k;
+          const int li = rank * LINES + i;
+          const long long r = row0 + li / LPR;
+          if (a.ahead > 0 && i < LINES && r < a.rows && (!CHIRP || (li % LPR) * 16 < a.n_in))
+            prefetch_l2(a.in + r * a.in_rs + (li % LPR) * 16);
+        }
       }
     }
     // W_N^{tr q} for q = 2q' + lane; groups g > 0 add the constant W_32^{g q}
