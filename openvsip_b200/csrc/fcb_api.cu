@@ -112,7 +112,10 @@ int check_device()
   cudaDeviceProp p;
   e = cudaGetDeviceProperties(&p, dev);
   if (e != cudaSuccess) return cuda_error(e, "cudaGetDeviceProperties");
-  if (p.major < 10) return set_error(FCB_ERR_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a", dev, p.major, p.minor);
+  // sm_100a code runs on compute capability 10.0 only
+  if (p.major != 10 || p.minor != 0)
+    return set_error(FCB_ERR_NODEVICE, "device %d is sm_%d%d; this library is built for sm_100a (compute capability 10.0)",
+                     dev, p.major, p.minor);
   return FCB_OK;
 }
 
