@@ -1,0 +1,40 @@
+"""bench.py's reference arm on the CPU: one JSON line with the metric, unit and
+direction of the GPU arm, the CPU baseline it measured and an e2e block with no
+host-device traffic; ranks other than 0 print nothing."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(env_extra, *args):
+    env = dict(os.environ, **env_extra)
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", *args],
+                          capture_output=True, text=True, env=env, timeout=600, cwd=ROOT)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_driver"))
+                    and not os.path.exists(os.path.join(ROOT, "oracle", "liboracle.so")),
+                    reason="neither the reference build nor the oracle library is built")
+def test_reference_arm_line():
+    r = _run({}, "--steps", "1", "--warmup", "1")
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["unit"] == "complex samples/s" and line["higher_is_better"] is True
+    assert line["value"] > 0 and line["steps"] == 1
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["cpu_baseline"]["value"] == line["value"] and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert "metric" in line and "config" in line and "workload" in line["config"]
+
+
+def test_reference_arm_other_ranks_print_nothing():
+    r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, "--steps", "1", "--warmup", "1")
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
