@@ -1,6 +1,7 @@
-"""bench.py's reference arm on the CPU: one JSON line with the metric, unit and
-direction of the GPU arm, the CPU baseline it measured and an e2e block with no
-host-device traffic; ranks other than 0 print nothing."""
+"""bench.py's output contract.  The reference arm (CPU): one JSON line with the
+metric, unit and direction of the GPU arm, the CPU baseline it measured and an
+e2e block with no host-device traffic; ranks other than 0 print nothing.  The
+GPU arm (on a B200): every key of its line, with consistent values."""
 import json
 import os
 import subprocess
@@ -38,3 +39,25 @@ def test_reference_arm_other_ranks_print_nothing():
     r = _run({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}, "--steps", "1", "--warmup", "1")
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == ""
+
+
+@pytest.mark.gpu
+def test_gpu_arm_line():
+    # a short run of the GPU arm on a smaller shape: every key of the line, with sane values
+    env = dict(os.environ)
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "5", "--warmup", "3",
+                        "--no-cpu-baseline", "--e2e-steps", "1", "--pulses", "64"],
+                       capture_output=True, text=True, env=env, timeout=900, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "roofline", "cpu_baseline", "e2e", "gpu_launches", "clocks"):
+        assert k in line, k
+    assert line["n_gpus"] == 1 and line["steps"] == 5 and line["warmup"] == 3 and line["gpu_launches"] == 5
+    assert line["value"] > 0 and line["higher_is_better"] is True and line["scaling"] == "weak"
+    roof = line["roofline"]
+    assert roof["bound"] == "hbm" and roof["unit"] == "GB/s" and 0 < roof["frac"] == roof["achieved"] / roof["peak"]
+    e2e = line["e2e"]
+    assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] == e2e["d2h_bytes_per_step"] == 64 * 16384 * 8
+    assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(line["clocks"])
+    assert line["rel_l2_vs_fp64"] <= 2e-6
