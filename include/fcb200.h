@@ -37,7 +37,10 @@
  *                                 Fftm+vmmul+Fftm jobs of uneven shapes in one
  *                                 persistent launch.
  *
- * Lengths: powers of two from 1 to 65536.
+ * Lengths: Fftm, fast-convolution and replica plans take any length from 1 to
+ * 32768 (lengths that are not powers of two run Bluestein's algorithm) and
+ * powers of two up to 65536; the batch entry points take powers of two from
+ * 256 to 32768; the 2-D plans take powers of two from 64 to 16384 per dimension.
  */
 #ifndef FCB200_H
 #define FCB200_H
@@ -191,10 +194,15 @@ FCB_API int fcb_replica_spectrum(const fcb_cf32 *replica_dev, long long n, int m
  * counterpart in the reference.  Its FP64 work buffers are a 2 MiB array built
  * into the library (held on every GPU that loads it until exit) instead of a
  * per-call allocation, so n is limited to 65536; larger n is rejected with
- * FCB_ERR_INVALID.  Asynchronous on `stream` (NULL: the default stream); it
+ * FCB_ERR_INVALID.  Unlike fcb_replica_spectrum it runs the radix-2 FP64 FFT
+ * only: n must be a power of two, other lengths are rejected with
+ * FCB_ERR_UNSUPPORTED.  Asynchronous on `stream` (NULL: the default stream); it
  * calls no allocator.  The first call on a device looks up the array's device
  * address (cudaGetSymbolAddress), so make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * capture; the address is kept per device for its primary context (the CUDA
+ * runtime's).  All calls share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU (different streams or threads) race,
+ * so serialise them, e.g. on one stream. */
 FCB_API int fcb_replica_spectrum_noalloc(const fcb_cf32 *replica_dev, long long n, int matched,
                                          fcb_cf32 *spectrum_dev, void *stream);
 

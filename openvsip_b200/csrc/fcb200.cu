@@ -484,7 +484,10 @@ double2 *g_noalloc_ptr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device.  The first call
 // on each device looks it up with cudaGetSymbolAddress (host code cannot use
-// the array's name as a device address).
+// the array's name as a device address).  The address is cached per device
+// ordinal, i.e. for the device's primary context, which is the context the
+// CUDA runtime uses; callers that switch to contexts of their own made with the
+// driver API are not supported by this entry point.
 int noalloc_scratch(double2 **out)
 {
   int dev = 0;
@@ -507,11 +510,13 @@ int noalloc_scratch(double2 **out)
 extern "C" FCB_API int fcb_replica_spectrum_noalloc(const fcb_cf32 *replica_dev, long long n, int matched,
                                                     fcb_cf32 *spectrum_dev, void *stream)
 {
-  if (n < 1 || (n & (n - 1)) != 0)
-    return fcb::set_error(FCB_ERR_UNSUPPORTED, "length %lld is not a power of two", n);
+  // the size limit first: any n above it is FCB_ERR_INVALID, power of two or not
   if (n > kNoAllocMaxN)
     return fcb::set_error(FCB_ERR_INVALID, "length %lld exceeds the no-allocation scratch limit of %lld samples",
                           n, kNoAllocMaxN);
+  if (n < 1 || (n & (n - 1)) != 0)
+    return fcb::set_error(FCB_ERR_UNSUPPORTED, "length %lld is not a power of two (the no-allocation entry point "
+                          "runs the radix-2 FP64 FFT only)", n);
   if (!replica_dev || !spectrum_dev) return fcb::set_error(FCB_ERR_INVALID, "NULL pointer");
   double2 *scratch = nullptr;
   int rc = noalloc_scratch(&scratch);

@@ -31,7 +31,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# the reference checkout: the argument, else $OPENVSIP_REF, else a directory
+# named "reference" beside this repository
+REF = (sys.argv[1] if len(sys.argv) > 1 else None) or os.environ.get("OPENVSIP_REF") or \
+    os.path.join(os.path.dirname(ROOT), "reference")
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 
 
