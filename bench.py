@@ -10,7 +10,11 @@ step, larger than the 126 MB L2; two input buffers alternate).
 
 N > 1 is launched by torchrun (one rank per GPU); every rank runs its own
 batch (weak scaling, no data-path collective), timing is the max over ranks.
-Prints one JSON line on rank 0.
+Prints one JSON line on rank 0.  Besides the headline it carries blocks for
+the phased Impl1op form on the same data ("phased"), the uneven batch of 512
+jobs in one persistent launch per step with its jobs partitioned across ranks
+("batch"), and, on one GPU, the served Poisson stream ("serve"); --no-batch /
+--no-serve leave those out.
 """
 from __future__ import annotations
 
@@ -119,6 +123,29 @@ def dist_setup():
     return world, rank, local
 
 
+def host_info():
+    """The GPU box's host: CPU model and thread count (lscpu / os), and whether
+    the reference's production FFT library (FFTW3, single precision) is
+    installed -- the library and its header are probed, neither is assumed."""
+    import ctypes.util
+    import glob
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    headers = []
+    for d in ("/usr/include", "/usr/local/include", "/opt/*/include", sys.prefix + "/include"):
+        headers += glob.glob(os.path.join(d, "fftw3.h"))
+    lib = ctypes.util.find_library("fftw3f")
+    return {"cpu_model": model, "nproc": os.cpu_count(), "fftw3f_library": lib, "fftw3_header": headers[0] if
+            headers else None, "fftw3_usable": bool(lib and headers)}
+
+
 def cpu_reference_sample(rows_per_proc: int = 1):
     """The reference library's own CPU path (oracle/_ref, generic DFT backend --
     FFTW3 is not installed) on a bounded sample: nproc processes, each running
@@ -160,22 +187,31 @@ def cpu_port_sample():
             "sample": f"{rows} rows x {NSAMP} samples, oracle FP32 radix-2 port, {cores} threads"}
 
 
-def fftw_standin():
-    """scipy.fft complex64 (pocketfft) with all workers: a labelled stand-in for
-    the reference's FFTW3 FP32 path, which is not installed."""
+def rel_l2(y, ref):
+    y = np.asarray(y, dtype=np.complex128)
+    ref = np.asarray(ref, dtype=np.complex128)
+    return float(np.linalg.norm(y - ref) / np.linalg.norm(ref))
+
+
+def fftw_standin(x, spec, ref):
+    """scipy.fft complex64 (pocketfft) fft -> multiply -> ifft with all
+    workers: a labelled stand-in for the reference's FFTW3 FP32 path, which is
+    not installed.  x: rows of the workload (complex64), spec: the complex64
+    replica spectrum, ref: the FP64 result of those rows.  Returns its
+    throughput and its own error against FP64 on the same rows as the GPU's."""
     import scipy.fft
     cores = os.cpu_count() or 1
-    rows = 256
-    rng = np.random.default_rng(0)
-    x = (rng.standard_normal((rows, NSAMP)) + 1j * rng.standard_normal((rows, NSAMP))).astype(np.complex64)
-    rep = np.ones(NSAMP, dtype=np.complex64)
-    scipy.fft.ifft(scipy.fft.fft(x[:8], axis=1, workers=cores) * rep, axis=1, workers=cores)
+    reps = max(1, 256 // x.shape[0])
+    xx = np.concatenate([x] * reps, axis=0)
+    scipy.fft.ifft(scipy.fft.fft(xx[:8], axis=1, workers=cores) * spec, axis=1, workers=cores)
     t0 = time.perf_counter()
     for _ in range(3):
-        scipy.fft.ifft(scipy.fft.fft(x, axis=1, workers=cores) * rep, axis=1, workers=cores)
+        scipy.fft.ifft(scipy.fft.fft(xx, axis=1, workers=cores) * spec, axis=1, workers=cores)
     wall = (time.perf_counter() - t0) / 3
-    return {"value": rows * NSAMP / wall, "unit": "complex samples/s", "cores": cores,
-            "what": "scipy.fft complex64 fft -> multiply -> ifft, FFTW3 stand-in (not the reference)"}
+    y = scipy.fft.ifft(scipy.fft.fft(x, axis=1, workers=cores) * spec, axis=1, workers=cores)
+    return {"value": xx.shape[0] * x.shape[1] / wall, "unit": "complex samples/s", "cores": cores,
+            "rel_l2_vs_fp64": rel_l2(y.astype(np.complex64), ref), "rows_checked": int(x.shape[0]),
+            "what": "scipy.fft complex64 fft -> multiply -> ifft, FFTW3 FP32 stand-in (not the reference)"}
 
 
 # Wall-clock cap of the reference arm.  Its smallest step is one 16384-sample row per host
@@ -216,60 +252,84 @@ def run_reference(args, world, rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
             "config": {"workload": WORKLOAD + " (bounded sample per step)", "parallelism": f"{cores} host processes"},
             "cpu_baseline": {"value": value, "unit": "complex samples/s", "cores": cores, "kind": kind,
-                             "sample": steps[-1]["sample"]},
+                             "sample": steps[-1]["sample"], "host": host_info()},
             "e2e": {"value": value, "unit": "complex samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
+def _time_calls(fn, steps, stream):
+    """Mean milliseconds per call of fn over `steps` back-to-back calls (CUDA
+    events on `stream`, after 3 untimed calls)."""
+    import torch
+    for _ in range(3):
+        fn()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    for _ in range(steps):
+        fn()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    return ev[0].elapsed_time(ev[1]) / steps
+
+
+L2_BYTES = 126 << 20
+
+
 def run_sweep(args):
-    """Per-length throughput of the fused fast convolution and the forward row
-    Fftm (the 256 x {256..65536} sweep shape, and a fixed 2^24-sample batch per
-    length), one JSON line per (kind, length); kernel time by CUDA events."""
+    """Per-length throughput lines: the fused fast convolution, the phased
+    Impl1op form (Fftm -> vmmul -> Fftm, three launches; benchmarks/fastconv.cpp
+    :100-106) and the forward row Fftm, on three shapes: the reference
+    benchmark's 64 rows x 2^4 .. 2^16 (benchmarks/fastconv.cpp:977-988), the
+    256 x {256 .. 65536} row sweep, and a fixed 2^24-sample batch per length;
+    then the 4096 x 4096 2-D FFT.  Kernel time by CUDA events."""
     import torch
 
     import openvsip_b200 as ov
     torch.cuda.set_device(0)
     peak, _ = measured_peak()
     stream = torch.cuda.current_stream()
-    for logn in range(8, 17):
-        n = 1 << logn
-        for rows_label, rows in (("256 rows", 256), ("2^24 samples", (1 << 24) // n)):
-            x = (torch.randn(rows, n, dtype=torch.complex64, device="cuda"))
+    shapes = [("64 rows (reference benchmark shape)", 64, range(4, 17)), ("256 rows", 256, range(8, 17)),
+              ("2^24 samples", None, range(8, 17))]
+    for label, rows_fixed, logs in shapes:
+        for logn in logs:
+            n = 1 << logn
+            rows = rows_fixed or (1 << 24) // n
+            x = torch.randn(rows, n, dtype=torch.complex64, device="cuda")
             y = torch.empty_like(x)
-            rep = np.ones(n, dtype=np.complex64)
+            tmp = torch.empty_like(x)
+            rep_np = np.exp(2j * np.pi * np.random.default_rng(logn).random(n)).astype(np.complex64)
+            rep = torch.from_numpy(rep_np).cuda()
             if args.threads:
                 for kind_id in (0, 2):
                     ov.lib().fcb_tune_set(n, kind_id, args.threads)
-            for kind, plan in (("fastconv", ov.Fastconv(rep, rows)), ("fftm_fwd", ov.Fftm(rows, n, ov.fft_fwd))):
-                for _ in range(3):
-                    plan(x, y)
-                ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-                ev[0].record(stream)
-                for _ in range(args.steps):
-                    plan(x, y)
-                ev[1].record(stream)
-                torch.cuda.synchronize()
-                ms = ev[0].elapsed_time(ev[1]) / args.steps
-                alg = 16.0 * rows * n + (8.0 * n if kind == "fastconv" else 0.0)
+            fc = ov.Fastconv(rep_np, rows)
+            fwd = ov.Fftm(rows, n, ov.fft_fwd)
+            inv = ov.Fftm(rows, n, ov.fft_inv, 1.0 / n)
+
+            def phased():
+                fwd(x, tmp)
+                ov.vmmul(rep, tmp, tmp)
+                inv(tmp, y)
+
+            for kind, fn, bps in (("fastconv", lambda: fc(x, y), 16.0), ("phased", phased, 48.0),
+                                  ("fftm_fwd", lambda: fwd(x, y), 16.0)):
+                steps = args.steps if rows * n >= (1 << 20) else max(args.steps, 2000)
+                ms = _time_calls(fn, steps, stream)
+                alg = bps * rows * n + (8.0 * n if kind != "fftm_fwd" else 0.0)
                 gbs = alg / (ms / 1e3) / 1e9
-                print(json.dumps({"sweep": kind, "n": n, "rows": rows, "shape": rows_label, "ms": ms,
+                print(json.dumps({"sweep": kind, "n": n, "rows": rows, "shape": label, "ms": ms,
                                   "samples_per_s": rows * n / (ms / 1e3), "gbs": gbs, "frac": gbs / peak,
-                                  "threads": plan.info()["threads"], "cluster": plan.info()["cluster_ctas"]}),
+                                  "alg_bytes_per_sample": bps, "l2_resident": 16 * rows * n < L2_BYTES,
+                                  "launches_per_call": 3 if kind == "phased" else 1,
+                                  "threads": fc.info()["threads"], "cluster": fc.info()["cluster_ctas"]}),
                       flush=True)
+            del fc, fwd, inv
     # 4096 x 4096 2-D FFT, forward and inverse (two HBM passes each: 32 B/sample)
     x = torch.randn(4096, 4096, dtype=torch.complex64, device="cuda")
     y = torch.empty_like(x)
     for name, plan in (("fft2d_fwd", ov.Fft2d(4096, 4096, ov.fft_fwd)),
                        ("fft2d_inv", ov.Fft2d(4096, 4096, ov.fft_inv, 1.0 / 4096 ** 2))):
-        for _ in range(3):
-            plan(x, y)
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        ev[0].record(stream)
-        for _ in range(args.steps):
-            plan(x, y)
-        ev[1].record(stream)
-        torch.cuda.synchronize()
-        ms = ev[0].elapsed_time(ev[1]) / args.steps
+        ms = _time_calls(lambda: plan(x, y), args.steps, stream)
         gbs = 32.0 * 4096 * 4096 / (ms / 1e3) / 1e9
         print(json.dumps({"sweep": name, "n": 4096, "rows": 4096, "shape": "4096 x 4096", "ms": ms,
                           "samples_per_s": 4096 * 4096 / (ms / 1e3), "gbs": gbs, "frac": gbs / peak}), flush=True)
@@ -281,88 +341,136 @@ def _cgauss_dev(rows, n, gen):
     return torch.view_as_complex(x)  # sigma 1 per component
 
 
-def run_batch(args):
-    """Uneven batched fast convolution: 512 jobs, pulses ~ U{16..512}, samples
-    from {1024..32768}, each job with its own LFM replica (TBP ~ U[50, 1000]),
-    complex Gaussian inputs -- one persistent graph-replayed launch per step.
-    Prints one JSON line (not the headline benchmark)."""
+def fp64_fastconv(x, chirp64):
+    """FP64 reference (numpy): ifft(fft(x) * conj(fft(chirp))) per row."""
+    spec = np.conj(np.fft.fft(np.asarray(chirp64, dtype=np.complex128)))
+    return np.fft.ifft(np.fft.fft(np.asarray(x, dtype=np.complex128), axis=1) * spec, axis=1)
+
+
+BATCH_WORKLOAD = ("uneven batched fastconv, {jobs} jobs, pulses U{{16..512}}, samples from {{1024..32768}}, "
+                  "own LFM replica per job (TBP U[50,1000]), complex Gaussian inputs")
+
+
+def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> dict:
+    """The uneven batch (512 jobs, pulses U{16..512}, samples from
+    {1024..32768}, each job with its own LFM replica of TBP U[50, 1000],
+    complex Gaussian inputs): one persistent graph-replayed launch per step on
+    each rank.  With N ranks the jobs are partitioned by shard.partition_jobs
+    (balanced by samples; large jobs cut into pulse ranges), so the block
+    scales strongly.  Every job is checked against FP64 (numpy) on three of
+    its rows (first, middle, last of each rank's piece).  The plain per-call
+    GPU form (one fused Fastconv launch per job, plans made beforehand) is
+    timed on the same data."""
     import torch
 
-    from openvsip_b200 import autotune, synth
+    from openvsip_b200 import autotune, shard, synth
     from openvsip_b200.batch import Batch
     from openvsip_b200.vsip import Fastconv
-    torch.cuda.set_device(0)
     jobs = synth.uneven_jobs(seed=3, njobs=args.batch_jobs)
+    if world > 1:
+        mine = shard.partition_jobs([(j["pulses"], j["n"]) for j in jobs], world)[rank]
+    else:
+        mine = [(i, 0, j["pulses"]) for i, j in enumerate(jobs)]
     gen = torch.Generator(device="cuda")
-    gen.manual_seed(3)
-    xs = [_cgauss_dev(j["pulses"], j["n"], gen) for j in jobs]
+    xs, pieces = [], []
+    for ji, b, e in mine:
+        j = jobs[ji]
+        gen.manual_seed(int(j["seed"]))
+        xs.append(_cgauss_dev(j["pulses"], j["n"], gen)[b:e].contiguous())
+        pieces.append((ji, b, e))
     ys = [torch.empty_like(x) for x in xs]
-    chirps = [synth.job_replica(j).astype(np.complex64) for j in jobs]
-    samples = sum(j["pulses"] * j["n"] for j in jobs)
+    chirps = [synth.job_replica(jobs[ji]).astype(np.complex64) for ji, _, _ in pieces]
+    samples = sum(x.numel() for x in xs)
 
     def make(threads, order):
-        b = Batch(threads)
-        ids = [b.add_replica(c, kind="matched") for c in chirps]
-        b.set_jobs([(x, y, i) for x, y, i in zip(xs, ys, ids)], order=order)
-        return b
+        bt = Batch(threads)
+        ids = [bt.add_replica(c, kind="matched") for c in chirps]
+        bt.set_jobs([(x, y, i) for x, y, i in zip(xs, ys, ids)], order=order)
+        return bt
 
     tune = autotune.tune_batch(make, reps=3)
-    b = make(tune["threads"], tune["order"])
+    bt = make(tune["threads"], tune["order"])
     stream = torch.cuda.current_stream()
-    b.set_stream(stream.cuda_stream)
+    bt.set_stream(stream.cuda_stream)
     for _ in range(args.warmup):
-        b.run()
+        bt.run()
     torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(0) as clk:
+    # accuracy of every job (3 rows each) against FP64
+    errs = []
+    for (ji, b, e), x, y, c in zip(pieces, xs, ys, chirps):
+        rows = sorted({0, (e - b) // 2, e - b - 1})
+        ref = fp64_fastconv(x[rows].cpu().numpy(), c)
+        errs.append(rel_l2(y[rows].cpu().numpy(), ref))
+    steps = max(3, min(args.steps, 20))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    barrier()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        t0.record(stream)
         for s_, e_ in ev:
             s_.record(stream)
-            b.run()
+            bt.run()
             e_.record(stream)
+        t1.record(stream)
         torch.cuda.synchronize()
+    barrier()
+    total_ms = shard.max_over_ranks(t0.elapsed_time(t1))
     ms = [s_.elapsed_time(e_) for s_, e_ in ev]
-    mean = sum(ms) / len(ms)
-    alg = 16.0 * samples + 8.0 * sum(j["n"] for j in jobs)
-    peak, _ = measured_peak()
+    mean = total_ms / steps
+    all_samples = sum(j["pulses"] * j["n"] for j in jobs)
+    alg = 16.0 * all_samples + 8.0 * sum(j["n"] for j in jobs)
+    peak, peak_src = measured_peak()
     # the plain per-call GPU form: one fused launch per job, plans prepared beforehand
-    plans = [Fastconv(c, j["pulses"], kind="matched") for c, j in zip(chirps, jobs)]
-    for p_, x, y in zip(plans, xs, ys):
-        p_(x, y)
-    torch.cuda.synchronize()
-    s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s_.record(stream)
-    for p_, x, y in zip(plans, xs, ys):
-        p_(x, y)
-    e_.record(stream)
-    torch.cuda.synchronize()
-    per_call_ms = s_.elapsed_time(e_)
+    plans = [Fastconv(c, x.shape[0], kind="matched") for c, x in zip(chirps, xs)]
+    per_call_ms = shard.max_over_ranks(_time_calls(lambda: [p_(x, y) for p_, x, y in zip(plans, xs, ys)], 3, stream))
     srt = sorted(ms)
-    print(json.dumps({
-        "workload": f"uneven batched fastconv, {len(jobs)} jobs, pulses U{{16..512}}, samples from "
-                    f"{{1024..32768}}, own LFM replica per job", "samples_per_step": samples,
-        "value": samples / (mean / 1e3), "unit": "complex samples/s", "ms_per_step": mean,
+    max_err = shard.max_over_ranks(max(errs))
+    return {
+        "workload": BATCH_WORKLOAD.format(jobs=len(jobs)), "samples_per_step": all_samples,
+        "value": all_samples / (mean / 1e3), "unit": "complex samples/s", "ms_per_step": mean, "steps": steps,
+        "scaling": "strong" if world > 1 else None,
         "latency_ms": {"p50": srt[len(srt) // 2], "p99": srt[min(len(srt) - 1, int(0.99 * len(srt)))]},
         "roofline": {"bound": "hbm", "achieved": alg / (mean / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": alg / (mean / 1e3) / 1e9 / peak},
-        "tuning": tune, "batch": b.info(),
-        "per_call": {"ms": per_call_ms, "value": samples / (per_call_ms / 1e3),
+                     "frac": alg / (mean / 1e3) / 1e9 / peak, "peak_source": peak_src,
+                     "alg_bytes_per_step": alg},
+        "rel_l2_vs_fp64": {"max": max_err, "median_rank0": float(np.median(errs)), "jobs_checked": len(errs),
+                           "rows_per_job": 3, "tolerance": 2e-6},
+        "tuning": tune, "batch": bt.info(), "gpu_launches_per_step": 1,
+        "per_call": {"ms": per_call_ms, "value": all_samples / (per_call_ms / 1e3), "launches_per_step": len(plans),
                      "how": "one fused Fastconv launch per job, plans prepared beforehand, device data"},
-        "batch_over_per_call": per_call_ms / mean, "clocks": clk.summary()}), flush=True)
+        "batch_over_per_call": per_call_ms / mean, "clocks": clk.summary()}
 
 
-def run_serve(args):
+def run_batch(args):
+    """--batch: the uneven batch as a line of its own (not the headline)."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(batch_block(args)), flush=True)
+
+
+SERVE_WORKLOAD = ("served pulse compression, Poisson {rate:g} jobs/s for {seconds:g} s, uneven shapes, "
+                  "64 resident replicas, 40 GB admission budget")
+
+
+def serve_block(args) -> dict:
     """Served pulse-compression stream: Poisson arrivals at --serve-rate jobs/s
     for --serve-seconds, job shapes as in the uneven batch (pulses U{16..512},
     samples from {1024..32768}), 64 distinct replicas resident on the device,
     admission capped by a 40 GB device-memory budget.  Inputs are pre-staged on
     the device (a pool of complex Gaussian rows per length), so host<->device
-    transfers are not part of the latency.  Prints one JSON line with p50/p99
-    latency, throughput and per-job rel-L2 against FP64 on a sample of jobs."""
+    transfers are not part of the latency.  Every --serve-check-every-th job
+    (default: every job) is checked against FP64: the FP64 results of the
+    whole pool for every replica are computed on the host by numpy/scipy
+    before the stream starts, and each job's output is compared with its rows
+    on a separate CUDA stream while the stream runs."""
+    import queue
+
+    import scipy.fft
     import torch
 
     from openvsip_b200 import synth
     from openvsip_b200.serve import Server
-    torch.cuda.set_device(0)
     rng = np.random.default_rng(11)
     sizes = synth.SIZES
     replicas = []
@@ -374,25 +482,42 @@ def run_serve(args):
     gen.manual_seed(11)
     pool = {n: _cgauss_dev(512, n, gen) for n in sizes}
     torch.cuda.synchronize()
+    # FP64 results of every pool row for every replica (host numpy/scipy, then resident on the device)
+    cores = os.cpu_count() or 1
+    refs, ref_cum = [], []
+    pool_f = {n: scipy.fft.fft(pool[n].cpu().numpy().astype(np.complex128), axis=1, workers=cores) for n in sizes}
+    for r in replicas:
+        spec = np.conj(np.fft.fft(r.astype(np.complex128)))
+        ref = scipy.fft.ifft(pool_f[r.size] * spec, axis=1, workers=cores)
+        ref_cum.append(np.cumsum(np.sum(np.abs(ref) ** 2, axis=1)))
+        refs.append(torch.from_numpy(ref).cuda())
+    del pool_f
+    torch.cuda.synchronize()
     rate, seconds = args.serve_rate, args.serve_seconds
     count = int(rng.poisson(rate * seconds))
     arrivals = np.sort(rng.uniform(0, seconds, count))
     shapes = [(int(rng.integers(16, 513)), int(sizes[int(rng.integers(0, len(sizes)))])) for _ in range(count)]
-    import queue
+    rids = [by_n[n][int(rng.integers(0, len(by_n[n])))] for _, n in shapes]
     done_q = queue.Queue()
-    lat, checked, t_arrive = [], [], []
-    every = max(1, count // 32)
+    lat, t_arrive = [], []
+    every = max(1, int(args.serve_check_every))
+    check_stream = torch.cuda.Stream()
+    nums, dens = [], []
 
     def consume():
-        # the client side: wait for each result in order, keep a sample for the
-        # FP64 check, release the rest (results are the client's memory)
+        # the client side: wait for each result in order; every `every`-th job
+        # is compared with its FP64 rows on the check stream
         for i in range(count):
             r, p, n, rid = done_q.get()
             r.wait(timeout=600)
             lat.append(r.latency)
             t_arrive.append(r.t_submit)
             if i % every == 0:
-                checked.append((r.out, p, n, rid))  # copied to the host after the stream
+                with torch.cuda.stream(check_stream):
+                    d = r.out.to(torch.complex128) - refs[rid][:p]
+                    nums.append(torch.linalg.vector_norm(d))
+                dens.append(float(np.sqrt(ref_cum[rid][p - 1])))
+                r.out.record_stream(check_stream)
             r.out = None
 
     consumer = threading.Thread(target=consume)
@@ -409,45 +534,68 @@ def run_serve(args):
         gc.disable()
         consumer.start()
         t0 = time.perf_counter()
-        for t_arr, (p, n) in zip(arrivals, shapes):
-            delay = t0 + t_arr - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            rid = by_n[n][int(rng.integers(0, len(by_n[n])))]
-            done_q.put((srv.submit(pool[n][:p], rid), p, n, rid))
-        consumer.join()
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            for t_arr, (p, n), rid in zip(arrivals, shapes, rids):
+                delay = t0 + t_arr - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                done_q.put((srv.submit(pool[n][:p], rid), p, n, rid))
+            consumer.join()
         wall = time.perf_counter() - t0
         gc.enable()
         launches = srv.launches
         issue_ms = np.array(srv.issue_times) * 1e3
-        worst = sorted(srv.issue_parts, key=lambda v: -sum(v[:3]))[:5]
+    check_stream.synchronize()
+    errs = (torch.stack(nums).cpu().numpy() / np.array(dens)) if nums else np.array([np.nan])
     lat = np.array(lat) * 1e3
-    sec = (np.array(t_arrive) - t0).astype(int)
-    by_sec = {int(k): float(np.percentile(lat[sec == k], 99)) for k in np.unique(sec)}
     samples = sum(p * n for p, n in shapes)
-    # rel-L2 against FP64 (numpy) on a sample of jobs
-    errs = []
-    for y, p, n, rid in checked:
-        x = pool[n][:p].cpu().numpy().astype(np.complex128)
-        spec = np.conj(np.fft.fft(replicas[rid].astype(np.complex128)))
-        ref = np.fft.ifft(np.fft.fft(x, axis=1) * spec, axis=1)
-        y = y.cpu().numpy()
-        errs.append(float(np.linalg.norm(y.astype(np.complex128) - ref) / np.linalg.norm(ref)))
-    print(json.dumps({
-        "workload": f"served pulse compression, Poisson {rate:g} jobs/s for {seconds:g} s, uneven shapes, "
-                    f"64 resident replicas, 40 GB admission budget", "jobs": count, "launches": launches,
+    return {
+        "workload": SERVE_WORKLOAD.format(rate=rate, seconds=seconds), "jobs": count, "launches": launches,
         "offered_samples_per_s": samples / seconds, "value": samples / wall, "unit": "complex samples/s",
+        "wall_s": wall,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max())},
-        "rel_l2_vs_fp64": {"max": max(errs), "median": float(np.median(errs)), "jobs_checked": len(errs)},
-        "p99_latency_ms_by_arrival_second": by_sec,
+        "rel_l2_vs_fp64": {"max": float(errs.max()), "median": float(np.median(errs)), "jobs_checked": int(errs.size),
+                           "check_every": every, "tolerance": 2e-6,
+                           "how": "FP64 numpy/scipy result of each job's rows, compared on a side CUDA stream"},
         "host_issue_ms_per_launch": {"p50": float(np.percentile(issue_ms, 50)),
-                                     "p99": float(np.percentile(issue_ms, 99)), "max": float(issue_ms.max()),
-                                     "slowest_alloc_table_launch_ms_jobs": [[round(a * 1e3, 3), round(b_ * 1e3, 3),
-                                                                             round(c * 1e3, 3), n_]
-                                                                            for a, b_, c, n_ in worst]},
-        "inputs": "pre-staged on the device; latency is submit -> completion observed by the scheduler"}),
-        flush=True)
+                                     "p99": float(np.percentile(issue_ms, 99)), "max": float(issue_ms.max())},
+        "clocks": clk.summary(),
+        "inputs": "pre-staged on the device; latency is submit -> completion observed by the scheduler"}
+
+
+def run_serve(args):
+    """--serve: the served stream as a line of its own (not the headline)."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(serve_block(args)), flush=True)
+
+
+def phased_block(ov, x, y, chirp_dev, pulses, nsamp, steps, stream) -> dict:
+    """The reference benchmark's Impl1op form (benchmarks/fastconv.cpp:100-106)
+    on the GPU: forward Fftm, vmmul<0> by the replica spectrum, inverse Fftm
+    scaled by 1/N -- three launches and three HBM round trips per step (48 B
+    per sample of algorithmic traffic), on the same device data as the fused
+    headline."""
+    import torch
+    spec = ov.replica_spectrum(chirp_dev, matched=True)
+    tmp = torch.empty_like(y)
+    fwd = ov.Fftm(pulses, nsamp, ov.fft_fwd)
+    inv = ov.Fftm(pulses, nsamp, ov.fft_inv, 1.0 / nsamp)
+
+    def step():
+        fwd(x, tmp)
+        ov.vmmul(spec, tmp, tmp)
+        inv(tmp, y)
+
+    ms = _time_calls(step, steps, stream)
+    alg = 48.0 * pulses * nsamp + 8.0 * nsamp
+    peak, _ = measured_peak()
+    return {"form": "Impl1op: Fftm(fwd) -> vmmul<0> -> Fftm(inv, 1/N), three launches per step",
+            "value": pulses * nsamp / (ms / 1e3), "unit": "complex samples/s", "ms_per_step": ms, "steps": steps,
+            "roofline": {"bound": "hbm", "alg_bytes_per_step": alg, "achieved": alg / (ms / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak},
+            "gpu_launches_per_step": 3}
 
 
 def main():
@@ -457,6 +605,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="fcb", choices=["fcb", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="leave the uneven-batch block out of the line")
+    ap.add_argument("--no-serve", action="store_true", help="leave the served-stream block out of the line")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--threads", type=int, default=0, help="force the 256- or 512-thread kernel variant")
     ap.add_argument("--sweep", action="store_true", help="per-length throughput lines instead of the benchmark")
@@ -464,7 +614,8 @@ def main():
     ap.add_argument("--batch-jobs", type=int, default=512)
     ap.add_argument("--serve", action="store_true", help="served-stream line instead of the benchmark")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
-    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
+    ap.add_argument("--serve-check-every", type=int, default=1)
     ap.add_argument("--pulses", type=int, default=PULSES, help="override the pulse count (profiling other shapes)")
     ap.add_argument("--samples", type=int, default=NSAMP, help="override the samples per pulse")
     args = ap.parse_args()
@@ -501,8 +652,10 @@ def main():
         ov.lib().fcb_tune_set(nsamp, 2, args.threads)
     job = synth.large_fastconv(seed=1000 + rank, pulses=pulses, n=nsamp, tbp=TBP, echoes=ECHOES)
     x_host = job["data"]
-    rep = job["replica_spectrum"]
-    fc = ov.Fastconv(rep, pulses)
+    chirp = job["chirp"].astype(np.complex64)
+    # the replica spectrum is built by the library in FP64 on the GPU from the time-domain chirp
+    # (replica kind "matched": conj(FFT(chirp)))
+    fc = ov.Fastconv(chirp, pulses, kind="matched")
     info = fc.info()
     xin = [torch.from_numpy(x_host).cuda(), torch.from_numpy(np.roll(x_host, 1, axis=0)).cuda()]
     yout = torch.empty_like(xin[0])
@@ -519,10 +672,10 @@ def main():
     # accuracy of this run's output on a sample of rows (numpy FP64 FFT)
     fc(xin[0], yout)
     torch.cuda.synchronize()
-    ys = yout[:32].cpu().numpy().astype(np.complex128)
-    xs = x_host[:32].astype(np.complex128)
-    ref = np.fft.ifft(np.fft.fft(xs, axis=1) * rep.astype(np.complex128), axis=1)
-    rel = float(np.linalg.norm(ys - ref) / np.linalg.norm(ref))
+    check_rows = min(32, pulses)
+    ys = yout[:check_rows].cpu().numpy()
+    ref = fp64_fastconv(x_host[:check_rows], chirp)
+    rel = rel_l2(ys, ref)
 
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
@@ -558,6 +711,10 @@ def main():
     achieved = alg_bytes / (launch_ms / 1e3) / 1e9
     peak, peak_src = measured_peak()
 
+    # the phased Impl1op form on the same device data
+    phased = phased_block(ov, xin[0], yout, torch.from_numpy(chirp).cuda(), pulses, nsamp, min(args.steps, 50),
+                          stream)
+
     # end to end through the public API with pinned host buffers
     hin = torch.from_numpy(x_host).pin_memory().numpy()
     hout = torch.empty(x_host.shape, dtype=torch.complex64).pin_memory().numpy()
@@ -570,13 +727,19 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_value = samples_step * e2e_steps * world / shard.max_over_ranks(e2e_s)
 
+    # the uneven batch on every rank (jobs partitioned across ranks), the served stream on one GPU
+    batch = None if args.no_batch else batch_block(args, world, rank, barrier)
+    serve = serve_block(args) if (world == 1 and not args.no_serve) else None
+
     if rank == 0:
         cpu = None
         standin = None
         if world == 1 and not args.no_cpu_baseline:
             cpu = cpu_reference_sample(1) or cpu_port_sample()
             cpu.pop("seconds", None)
-            standin = fftw_standin()
+            cpu["host"] = host_info()
+            standin = fftw_standin(x_host[:check_rows], np.conj(np.fft.fft(chirp.astype(np.complex128))).astype(
+                np.complex64), ref)
         sorted_ms = sorted(step_ms)
         line = {
             "metric": baseline_metric(), "value": value, "unit": "complex samples/s", "n_gpus": world,
@@ -586,6 +749,7 @@ def main():
             "config": {"workload": WORKLOAD if default_shape else WORKLOAD.replace(
                            f"{PULSES} pulses x {NSAMP} samples", f"{pulses} pulses x {nsamp} samples"),
                        "pulses": pulses, "samples": nsamp, "tbp": TBP,
+                       "replica": "time-domain chirp, spectrum built by the library in FP64 on the GPU (matched)",
                        "parallelism": f"{world} independent batches (weak)",
                        "l2": f"inputs larger than L2 ({16 * samples_step >> 20} MB read+write per step, "
                              "2 alternating inputs)",
@@ -596,6 +760,7 @@ def main():
                            "p99": sorted_ms[min(len(sorted_ms) - 1, int(0.99 * len(sorted_ms)))],
                            "launches": lat_steps},
             "rel_l2_vs_fp64": rel,
+            "rel_l2_rows_checked": check_rows,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": ncu_traffic() if default_shape else None,
                          "peak_source": peak_src,
@@ -605,6 +770,9 @@ def main():
             "e2e": {"value": e2e_value, "unit": "complex samples/s", "h2d_bytes_per_step": x_host.nbytes,
                     "d2h_bytes_per_step": x_host.nbytes, "steps": e2e_steps,
                     "how": "Fastconv(host pinned in, host pinned out): chunked H2D / kernel / D2H on three streams"},
+            "phased": phased,
+            "batch": batch,
+            "serve": serve,
             "gpu_launches": args.steps,
             "clocks": clk.summary(),
         }

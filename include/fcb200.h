@@ -40,7 +40,7 @@
  * Lengths: Fftm, fast-convolution and replica plans take any length from 1 to
  * 32768 (lengths that are not powers of two run Bluestein's algorithm) and
  * powers of two up to 65536; the batch entry points take powers of two from
- * 256 to 32768; the 2-D plans take powers of two from 64 to 16384 per dimension.
+ * 256 to 32768; the 2-D plans take any supported length per dimension.
  */
 #ifndef FCB200_H
 #define FCB200_H
@@ -130,12 +130,15 @@ FCB_API int fcb_exec_r2c(fcb_plan plan, const float *in, long long in_rs, fcb_cf
 FCB_API int fcb_exec_c2r(fcb_plan plan, const fcb_cf32 *in, long long in_rs, float *out,
                          long long out_rs, long long rows, int where);
 
-/* 2-D FFT plan over a rows x cols matrix (both powers of two in [64, 16384]),
- * output times scale; fcb_exec then takes rows == the plan's rows.  Replaces
- * fft_backend<2, complex<float>, complex<float>, S> (src/ovxx/signal/fft/
- * backend.hpp:294-375; FFTW 2-D plan src/ovxx/fftw/fftw.cpp:436-511), used by
- * vsip::Fft<const_Matrix, ...>.  Two passes, each a row transform that stores
- * its result transposed; the plan keeps one rows x cols scratch matrix. */
+/* 2-D FFT plan over a rows x cols matrix, output times scale; fcb_exec then
+ * takes rows == the plan's rows.  Replaces fft_backend<2, complex<float>,
+ * complex<float>, S> (src/ovxx/signal/fft/backend.hpp:294-375; FFTW 2-D plan
+ * src/ovxx/fftw/fftw.cpp:436-511), used by vsip::Fft<const_Matrix, ...>.
+ * Both dimensions powers of two in [64, 16384]: two passes, each a row
+ * transform that stores its result transposed (one rows x cols scratch
+ * matrix).  Other dimensions (each any length fcb_supported_length accepts):
+ * a row pass, a transpose, a column pass and a transpose back (two scratch
+ * matrices). */
 FCB_API int fcb_plan_fft2d(long long rows, long long cols, int exponent, float scale,
                            fcb_plan *plan);
 

@@ -202,6 +202,28 @@ __global__ void vmmul_kernel(const float2 *v, const float2 *m, long long m_rs, f
   }
 }
 
+// out[c][r] = in[r][c] for a rows x cols matrix, through 32 x 32 tiles in
+// shared memory (coalesced reads and writes); one CTA of 32 x 8 threads per
+// tile.  Used by 2-D FFT plans whose sizes the transposing row kernels do not
+// cover.
+__global__ void transpose_kernel(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
+                                 long long cols)
+{
+  __shared__ float2 tile[32][33];
+  const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += 8)
+  {
+    const long long r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = in[r * in_rs + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += 8)
+  {
+    const long long c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[c * out_rs + r] = tile[threadIdx.x][k];
+  }
+}
+
 // Length-1 rows: out = in * w (w = scale, or the replica value).
 __global__ void scale_rows_kernel(const float2 *in, long long in_rs, float2 *out, long long out_rs,
                                   long long rows, const float4 *rep, long long rep_rs, float scale)
@@ -442,6 +464,18 @@ int launch_vmmul(const float2 *v, const float2 *m, long long m_rs, float2 *out, 
   vmmul_kernel<<<(unsigned)blocks, 256, 0, st>>>(v, m, m_rs, out, out_rs, rows, cols);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_error(e, "vmmul launch");
+  return FCB_OK;
+}
+
+int launch_transpose(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
+                     long long cols, cudaStream_t st)
+{
+  if (rows <= 0 || cols <= 0) return FCB_OK;
+  const long long gx = (cols + 31) / 32, gy = (rows + 31) / 32;
+  if (gy > 65535 || gx > 0x7fffffffLL) return set_error(FCB_ERR_INVALID, "matrix too large to transpose");
+  transpose_kernel<<<dim3((unsigned)gx, (unsigned)gy), dim3(32, 8), 0, st>>>(in, in_rs, out, out_rs, rows, cols);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_error(e, "transpose launch");
   return FCB_OK;
 }
 

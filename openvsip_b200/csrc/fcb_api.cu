@@ -43,6 +43,12 @@ struct fcb_plan_s
   float4 *twc = nullptr;
   float2 *scratch = nullptr;
   float2 *stage2d_in = nullptr, *stage2d_out = nullptr;
+  // 2-D FFT of other sizes (any dimensions the row plans support): a row plan
+  // of length cols, a transpose, a row plan of length rows on the transposed
+  // matrix, and a transpose back; scratch2 holds the transposed matrix.
+  bool general2d = false;
+  fcb_plan sub2d[2] = {nullptr, nullptr};
+  float2 *scratch2 = nullptr;
   // Rows of non-power-of-two length n (Bluestein): the fused kernel's
   // kChirpconv mode runs on work rows of blue_m >= 2n - 1 samples, reading the
   // n samples times a chirp (zero beyond) and writing n samples times a chirp.
@@ -131,6 +137,9 @@ void plan_free(fcb_plan p)
   cudaFree(p->scratch);
   cudaFree(p->stage2d_in);
   cudaFree(p->stage2d_out);
+  cudaFree(p->scratch2);
+  plan_free(p->sub2d[0]);
+  plan_free(p->sub2d[1]);
   cudaFree(p->rep);
   for (auto b : p->stage) cudaFree(b);
   for (int d = 0; d < 2; ++d)
@@ -460,6 +469,15 @@ int exec_real(fcb_plan p, int kind, const void *in, long long in_rs, void *out, 
 // 2-D FFT on device pointers: two transposing row passes.
 int exec_2d(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs, cudaStream_t st)
 {
+  if (p->general2d)
+  {
+    const long long R = p->rows2d, C = p->cols2d;
+    int rc = exec_device(p->sub2d[0], in, in_rs, p->scratch, C, R, 0, st);
+    if (!rc) rc = launch_transpose(p->scratch, C, p->scratch2, R, R, C, st);        // scratch2 = scratch^T
+    if (!rc) rc = exec_device(p->sub2d[1], p->scratch2, R, p->scratch2, R, C, 0, st);  // the columns, scaled
+    if (!rc) rc = launch_transpose(p->scratch2, R, out, out_rs, C, R, st);
+    return rc;
+  }
   RowArgs a = {};
   a.in = in;
   a.in_rs = in_rs;
@@ -910,11 +928,41 @@ int fcb_plan_fft2d(long long rows, long long cols, int exponent, float scale, fc
 {
   if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
   *plan = nullptr;
+  if (exponent != FCB_FORWARD && exponent != FCB_INVERSE) return set_error(FCB_ERR_INVALID, "exponent must be -1 or +1");
   const int lr = log2_exact(rows), lc = log2_exact(cols);
   if (lr < 6 || lr > 14 || lc < 6 || lc > 14)
-    return set_error(FCB_ERR_UNSUPPORTED, "2-D FFT dimensions must be powers of two in [64, 16384], got %lld x %lld",
-                     rows, cols);
-  if (exponent != FCB_FORWARD && exponent != FCB_INVERSE) return set_error(FCB_ERR_INVALID, "exponent must be -1 or +1");
+  {
+    // other sizes: two row plans and two transposes (four passes)
+    if (rows < 1 || cols < 1 || !fcb_supported_length(rows) || !fcb_supported_length(cols))
+      return set_error(FCB_ERR_UNSUPPORTED, "2-D FFT dimensions %lld x %lld: each must be " FCB_LENGTH_RULE, rows,
+                       cols);
+    int rc = check_device();
+    if (rc) return rc;
+    fcb_plan p = new (std::nothrow) fcb_plan_s;
+    if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
+    cudaGetDevice(&p->device);
+    p->n = cols;
+    p->logn = -1;
+    p->mode = exponent == FCB_FORWARD ? kFwd : kInv;
+    p->rows_max = rows;
+    p->scale = scale;
+    p->is2d = p->general2d = true;
+    p->rows2d = rows;
+    p->cols2d = cols;
+    cudaError_t e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = cuda_error(e, "cudaStreamCreate");
+    p->stream = p->own_stream;
+    if (!rc) rc = fcb_plan_fftm(cols, rows, exponent, 1.f, &p->sub2d[0]);
+    if (!rc) rc = fcb_plan_fftm(rows, cols, exponent, scale, &p->sub2d[1]);
+    const size_t bytes = sizeof(float2) * (size_t)(rows * cols);
+    if (!rc && (e = cudaMalloc(&p->scratch, bytes)) != cudaSuccess)
+      rc = set_error(FCB_ERR_NOMEM, "2-D scratch: %s", cudaGetErrorString(e));
+    if (!rc && (e = cudaMalloc(&p->scratch2, bytes)) != cudaSuccess)
+      rc = set_error(FCB_ERR_NOMEM, "2-D scratch: %s", cudaGetErrorString(e));
+    if (rc) { plan_free(p); return rc; }
+    *plan = p;
+    return FCB_OK;
+  }
   fcb_plan p = new (std::nothrow) fcb_plan_s;
   if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
   const int mode = exponent == FCB_FORWARD ? kFwd : kInv;

@@ -53,6 +53,9 @@ int replica_spectrum_dev(const float2 *rep_dev, long long n, int matched, float2
                          cudaStream_t st);
 int launch_vmmul(const float2 *v, const float2 *m, long long m_rs, float2 *out, long long out_rs,
                  long long rows, long long cols, cudaStream_t st);
+// out[c][r] = in[r][c], rows x cols (strides in complex elements)
+int launch_transpose(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
+                     long long cols, cudaStream_t st);
 int launch_scale_rows(const float2 *in, long long in_rs, float2 *out, long long out_rs, long long rows,
                       const float4 *rep, long long rep_rs, float scale, cudaStream_t st);
 

@@ -1,7 +1,7 @@
 // OpenVSIP plugin that routes the fast-convolution path to the B200 backend
 // (libfcb200.so, C ABI in include/fcb200.h).  Include it (or pass it with
 // -include) before any code that constructs a vsip::Fftm; link -lfcb200.
-// No reference header is modified: the plugin fills two dispatch slots the
+// No reference header is modified: the plugin fills dispatch slots the
 // reference already reserves.
 //
 //  1. be::user for op::fftm<complex<float>, complex<float>, row | col, D, R, N>
@@ -38,6 +38,10 @@
 // raised through OVXX_DO_THROW, as the base-class backends do for
 // unimplemented paths.  A missing GPU is an error at construction, not a
 // silent fall back.
+//
+//  3. be::user for op::fft<2, complex<float>, complex<float>, S> (the 2-D
+//     vsip::Fft<const_Matrix, ...>; backend contract src/ovxx/signal/fft/
+//     backend.hpp:294-375), through fcb_plan_fft2d.
 //
 // Environment: FCB200_DEVICE selects the CUDA device (default 0);
 // FCB200_TRACE=1 prints one line per backend constructed and per fused call.
@@ -386,10 +390,92 @@ fftm<fft_inv> *as_inv(F const &functor)
   return const_cast<fftm<fft_inv> *>(dynamic_cast<fftm<fft_inv> const *>(&functor.backend()));
 }
 
+/// fft_backend for the 2-D complex<float> FFT (vsip::Fft<const_Matrix, C, C,
+/// S>) on the B200, the contract of src/ovxx/signal/fft/backend.hpp:294-375.
+/// It asks for dense row-major interleaved data (the DDA layer copies anything
+/// else), applies the scale itself (supports_scale() == true, so the
+/// workspace's scale pass, src/ovxx/signal/fft/workspace.hpp:474-478, is
+/// skipped) and runs in place or out of place through fcb_plan_fft2d.
+template <int S>
+class fft2d : public signal::fft::fft_backend<2, ctype, ctype, S>
+{
+public:
+  fft2d(Domain<2> const &dom, float scale) : rows_(dom[0].size()), cols_(dom[1].size()), plan_(0)
+  {
+    ensure_device();
+    check(fcb_plan_fft2d((long long)rows_, (long long)cols_, S == fft_fwd ? FCB_FORWARD : FCB_INVERSE, scale,
+                         &plan_));
+    if (trace())
+      std::fprintf(stderr, "[fcb200] Fft<2,%s> %lu x %lu scale %g on the B200\n", S == fft_fwd ? "fwd" : "inv",
+                   (unsigned long)rows_, (unsigned long)cols_, (double)scale);
+  }
+  ~fft2d()
+  {
+    if (plan_) fcb_destroy(plan_);
+  }
+  virtual bool supports_scale() { return true; }
+  virtual void query_layout(Rt_layout<2> &inout)
+  {
+    inout.packing = dense;
+    inout.order = tuple<0, 1, 2>();
+    inout.storage_format = array;
+  }
+  virtual void query_layout(Rt_layout<2> &in, Rt_layout<2> &out)
+  {
+    query_layout(in);
+    out = in;
+  }
+  virtual bool requires_copy(Rt_layout<2> &) { return false; }
+  virtual void in_place(ctype *inout, stride_type r, stride_type c, length_type rows, length_type cols)
+  {
+    run(inout, r, c, inout, r, c, rows, cols);
+  }
+  virtual void out_of_place(ctype *in, stride_type ir, stride_type ic, ctype *out, stride_type o_r,
+                            stride_type oc, length_type rows, length_type cols)
+  {
+    run(in, ir, ic, out, o_r, oc, rows, cols);
+  }
+
+private:
+  void run(ctype *in, stride_type ir, stride_type ic, ctype *out, stride_type o_r, stride_type oc,
+           length_type rows, length_type cols)
+  {
+    OVXX_PRECONDITION(ic == 1 && oc == 1 && rows == rows_ && cols == cols_);
+    check(fcb_exec(plan_, reinterpret_cast<fcb_cf32 const *>(in), rows > 1 ? ir : cols,
+                   reinterpret_cast<fcb_cf32 *>(out), rows > 1 ? o_r : cols, (long long)rows, FCB_HOST));
+  }
+
+  length_type rows_, cols_;
+  fcb_plan plan_;
+};
+
 } // namespace ovxx::fcb200
 
 namespace dispatcher
 {
+
+/// 2-D complex<float> Fft on the B200 (be::user slot, the first entry of
+/// List<op::fft> in src/ovxx/signal/fft.hpp:41-49).  Any dimensions the row
+/// plans support; other sizes fail rt_valid and fall through to the next
+/// backend in the list.
+template <int S, vsip::return_mechanism_type R, unsigned N>
+struct Evaluator<op::fft<2, std::complex<float>, std::complex<float>, S, R, N>, be::user,
+                 std::unique_ptr<signal::fft::fft_backend<2, std::complex<float>, std::complex<float>, S> >
+                 (Domain<2> const &, float)>
+{
+  typedef signal::fft::fft_backend<2, std::complex<float>, std::complex<float>, S> backend_type;
+  static bool const ct_valid = true;
+  static char const *name() { return "fcb200 fft 2-D (B200)"; }
+  static bool rt_valid(Domain<2> const &dom, float)
+  {
+    return dom[0].size() > 0 && dom[1].size() > 0 && fcb_supported_length((long long)dom[0].size()) &&
+           fcb_supported_length((long long)dom[1].size());
+  }
+  static std::unique_ptr<backend_type> exec(Domain<2> const &dom, float scale)
+  {
+    return std::unique_ptr<backend_type>(new fcb200::fft2d<S>(dom, scale));
+  }
+};
 
 /// Row-wise complex<float> Fftm on the B200 (be::user slot).
 template <int D, vsip::return_mechanism_type R, unsigned N>

@@ -6,7 +6,9 @@
 // writes out_prefix.{phased,fused,fusedm}.bin: the phased Fftm -> vmmul -> Fftm
 // form (benchmarks/fastconv.cpp:100-106), the fused by-value expression
 // (tests/fastconv.cpp:204) and the matrix-of-coefficients expression with each
-// row's weights equal to the vector times (1 + row/ROWS).
+// row's weights equal to the vector times (1 + row/ROWS); and
+// out_prefix.{fft2d,fft2d_rt}.bin: the 2-D vsip::Fft of the input and the
+// inverse 2-D Fft (scale 1 / (ROWS COLS), by value) of that result.
 #include "ovxx_fcb200.hpp"
 
 #include <vsip/initfin.hpp>
@@ -70,6 +72,14 @@ int main(int argc, char **argv)
     save(prefix + ".fused.bin", out);
     out = inv_fftm(wm * for_fftm(in));
     save(prefix + ".fusedm.bin", out);
+  }
+  {
+    Fft<const_Matrix, cf, cf, fft_fwd, by_reference> f2(Domain<2>(rows, cols), 1.0);
+    Fft<const_Matrix, cf, cf, fft_inv, by_value> g2(Domain<2>(rows, cols), 1.0 / (rows * cols));
+    f2(in, out);
+    save(prefix + ".fft2d.bin", out);
+    tmp = g2(out);
+    save(prefix + ".fft2d_rt.bin", tmp);
   }
   return 0;
 }

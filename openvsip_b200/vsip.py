@@ -254,7 +254,9 @@ class FftmReal(_Plan):
 class Fft2d(_Plan):
     """2-D FFT of a rows x cols matrix on the GPU (vsip::Fft<const_Matrix, C, C,
     D>, src/vsip/impl/signal/fft.hpp:75-132): rows, then columns, output times
-    scale.  Dimensions: powers of two in [64, 16384]."""
+    scale.  Dimensions: any supported row length (powers of two in [64, 16384]
+    take the two-pass transposing path, other sizes two row passes and two
+    transposes)."""
 
     def __init__(self, rows: int, cols: int, direction: int = fft_fwd, scale: float = 1.0):
         self.rows, self.cols = int(rows), int(cols)

@@ -89,3 +89,46 @@ def test_batch_rejects_bad_jobs():
         b.set_jobs([(x, x, rid)])  # replica length != row length
     with pytest.raises(FcbError):
         b.add_replica(np.ones(65536, dtype=np.complex64))  # beyond the batch's 32768
+
+
+def test_c3_full_config_every_job_vs_fp64(oracle):
+    """The full uneven batch: 512 jobs, pulses U{16..512}, samples from
+    {1024..32768}, each job with its own LFM replica (TBP U[50, 1000]), about
+    1.45 G samples in one persistent launch.  Every job is checked against the
+    FP64 oracle on three seeded rows (first, a random one, last), after two
+    replays of the graph (the second must be bit-identical to the first)."""
+    import torch
+    jobs = synth.uneven_jobs(seed=3, njobs=512)
+    gen = torch.Generator(device="cuda")
+    b = Batch()
+    xs, ys, chirps, jl = [], [], [], []
+    for j in jobs:
+        gen.manual_seed(int(j["seed"]))
+        x = torch.view_as_complex(torch.randn(j["pulses"], j["n"], 2, device="cuda", generator=gen))
+        chirp = synth.job_replica(j).astype(np.complex64)
+        rid = b.add_replica(chirp, kind="matched")
+        y = torch.full_like(x, float("nan"))
+        xs.append(x)
+        ys.append(y)
+        chirps.append(chirp)
+        jl.append((x, y, rid))
+    b.set_jobs(jl)
+    assert b.info()["samples"] == sum(j["pulses"] * j["n"] for j in jobs) > 1_000_000_000
+    b.run()
+    b.sync()
+    rng = np.random.default_rng(3)
+    picks = [sorted({0, int(rng.integers(0, j["pulses"])), j["pulses"] - 1}) for j in jobs]
+    first = [y[r].cpu().numpy() for y, r in zip(ys, picks)]
+    b.run()
+    b.sync()
+    worst = 0.0
+    for k, (j, x, y, c, rows) in enumerate(zip(jobs, xs, ys, chirps, picks)):
+        got = y[rows].cpu().numpy()
+        np.testing.assert_array_equal(got, first[k])
+        spec = np.conj(np.fft.fft(c.astype(np.complex128))).astype(np.complex64)
+        want = oracle.fastconv(x[rows].cpu().numpy(), spec)
+        err = oracle.rel_l2(got, want)
+        worst = max(worst, err)
+        assert err <= RTOL, f"job {k} ({j['pulses']} x {j['n']}): rel-L2 {err:.3e}"
+    # no job row was left unwritten (NaN-filled outputs)
+    assert all(bool(torch.isfinite(torch.view_as_real(y)).all()) for y in ys)

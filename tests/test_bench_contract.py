@@ -46,7 +46,8 @@ def test_gpu_arm_line():
     # a short run of the GPU arm on a smaller shape: every key of the line, with sane values
     env = dict(os.environ)
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "5", "--warmup", "3",
-                        "--no-cpu-baseline", "--e2e-steps", "1", "--pulses", "64"],
+                        "--no-cpu-baseline", "--e2e-steps", "1", "--pulses", "64", "--batch-jobs", "8",
+                        "--serve-seconds", "2", "--serve-rate", "100"],
                        capture_output=True, text=True, env=env, timeout=900, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
@@ -61,3 +62,11 @@ def test_gpu_arm_line():
     assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] == e2e["d2h_bytes_per_step"] == 64 * 16384 * 8
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(line["clocks"])
     assert line["rel_l2_vs_fp64"] <= 2e-6
+    ph = line["phased"]
+    assert ph["value"] > 0 and ph["gpu_launches_per_step"] == 3 and ph["roofline"]["frac"] > 0
+    b = line["batch"]
+    assert b["value"] > 0 and b["rel_l2_vs_fp64"]["max"] <= 2e-6 and b["rel_l2_vs_fp64"]["jobs_checked"] == 8
+    assert b["per_call"]["launches_per_step"] == 8 and b["batch_over_per_call"] > 0
+    sv = line["serve"]
+    assert sv["jobs"] > 0 and sv["rel_l2_vs_fp64"]["jobs_checked"] == sv["jobs"]
+    assert sv["rel_l2_vs_fp64"]["max"] <= 2e-6 and sv["latency_ms"]["p99"] >= sv["latency_ms"]["p50"] > 0

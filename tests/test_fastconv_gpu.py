@@ -130,3 +130,27 @@ def test_fastconv_full_size_pulse_compression(oracle):
     for p in range(4):
         for d, amp in zip(job["delays"][p], job["amplitudes"][p]):
             assert abs(y[p, int(d)]) > 0.5 * amp * n
+
+
+@pytest.mark.parametrize("case", ["C1", "C2"])
+def test_fastconv_accuracy_vs_fp32_cpu(oracle, case):
+    """The fused fast convolution's error is no worse than 2x the FP32 CPU
+    FFT's on the same seeded inputs: scipy's pocketfft complex64 stands in for
+    the reference's FFTW3 FP32 path, which is not installed.  C1: 64 pulses x
+    2048 samples, TBP 100; C2: 1024 pulses x 16384 samples with 8 echoes per
+    pulse, TBP 500.  Both with the spectrum given and with the time-domain
+    chirp transformed by the library in FP64 on the GPU."""
+    import scipy.fft
+    torch = _torch()
+    job = synth.cpu_case(seed=0) if case == "C1" else synth.large_fastconv(seed=1)
+    x, chirp = job["data"], job["chirp"].astype(np.complex64)
+    spec = np.conj(np.fft.fft(chirp.astype(np.complex128))).astype(np.complex64)
+    want = oracle.fastconv(x, spec)
+    cpu = scipy.fft.ifft(scipy.fft.fft(x, axis=1) * spec, axis=1)
+    assert cpu.dtype == np.complex64
+    cpu_err = oracle.rel_l2(cpu, want)
+    dx = torch.from_numpy(x).cuda()
+    for fc in (Fastconv(spec, x.shape[0]), Fastconv(chirp, x.shape[0], kind="matched")):
+        y = fc(dx).cpu().numpy()
+        err = oracle.rel_l2(y, want)
+        assert err <= RTOL and err <= 2 * cpu_err, (err, cpu_err)

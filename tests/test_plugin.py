@@ -74,6 +74,19 @@ def test_reference_matched_filter_example_on_b200():
 
 
 @pytest.mark.gpu
+def test_reference_fft2d_test_on_b200():
+    # tests/fft2d.cpp: forward and inverse 2-D complex FFTs by reference, by
+    # value and in place, scales 1, 1/4 and 1/N, at 8 x 8 and at the sizes that
+    # are not powers of two (2 x 2, 1 x 1, 2 x 1, 4 x 8, 8 x 128, 5 x 7, 24 x 48,
+    # 1 x 5), each checked by the test itself at -100 dB
+    r = _run([_prog("fft2d_test")])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for shape in ("8 x 8", "5 x 7", "24 x 48", "8 x 128", "1 x 5"):
+        assert f"[fcb200] Fft<2,fwd> {shape}" in r.stderr, shape
+        assert f"[fcb200] Fft<2,inv> {shape}" in r.stderr, shape
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("name", ["fftm_unaligned", "fft_ip_subview", "fft_temp_view"])
 def test_reference_fftm_regressions_on_b200(name):
     # tests/regressions: unaligned and gapped rows in interleaved and split
@@ -102,3 +115,9 @@ def test_plugin_forms_match_oracle(oracle, tmp_path, rows, cols):
     ym = np.fromfile(tmp_path / "out.fusedm.bin", dtype=np.complex64).reshape(rows, cols)
     assert oracle.rel_l2(ym, oracle.fastconv(x, wm)) <= 2e-6
     assert r.stderr.count("fused fastconv") >= 2
+    # the 2-D vsip::Fft forward (by reference) and inverse (by value, scale 1 / (rows cols))
+    y2 = np.fromfile(tmp_path / "out.fft2d.bin", dtype=np.complex64).reshape(rows, cols)
+    assert oracle.rel_l2(y2, np.fft.fft2(x.astype(np.complex128))) <= 2e-6
+    rt = np.fromfile(tmp_path / "out.fft2d_rt.bin", dtype=np.complex64).reshape(rows, cols)
+    assert oracle.rel_l2(rt, x) <= 2e-6
+    assert f"[fcb200] Fft<2,fwd> {rows} x {cols}" in r.stderr and f"[fcb200] Fft<2,inv> {rows} x {cols}" in r.stderr
