@@ -8,8 +8,11 @@ What it chooses (measured on the device with CUDA events, never guessed):
   samples, two per SM) or 512 threads (16384 samples, one per SM; rows of 4096
   samples and more), or 256 threads with 64 samples each (value -256, rows of
   16384 samples).  Rows longer than one CTA's samples split over a
-  thread-block cluster.  The choice is installed with fcb_tune_set and applies
-  to plans made afterwards.
+  thread-block cluster.  For the fused fast convolution of 32768-sample rows
+  there is also -2, the split variant: one 256-thread CTA per row runs the
+  row as two 16384-sample halves (64 samples per thread), holding the waiting
+  half in tensor memory.  The choice is installed with fcb_tune_set and
+  applies to plans made afterwards.
 * For the batched launch: the same CTA size (which also fixes the cluster
   shape: 4 x 256 or 2 x 512 threads for 32768-sample rows) and the job order
   (longest rows first, or as given).
@@ -30,9 +33,10 @@ KINDS = {"forward": 0, "inverse": 1, "fastconv": 2}
 VARIANT_MIN_N = 256  # below this every length has only the 256-thread kernel
 
 
-def variants(n: int) -> tuple:
-    """Kernel variants the library has at row length n: CTA sizes with 32
-    samples per thread, and -256 (256 threads x 64 samples) at 16384."""
+def variants(n: int, kind: str = "forward") -> tuple:
+    """Kernel variants the library has at row length n for `kind`: CTA sizes
+    with 32 samples per thread, -256 (256 threads x 64 samples) at 16384, and
+    -2 (two 64-sample halves, tensor memory) for the fused kind at 32768."""
     out = [256]
     if 256 <= n <= 8192:
         out.insert(0, 128)
@@ -40,6 +44,8 @@ def variants(n: int) -> tuple:
         out.append(512)
     if n == 16384:
         out.append(-256)
+    if n == 32768 and kind == "fastconv":
+        out.append(-2)
     return tuple(out)
 
 
@@ -90,7 +96,7 @@ def tune_plans(lengths=(1024, 4096, 8192, 16384, 32768, 65536), kinds=tuple(KIND
         for n in lengths:
             if n < VARIANT_MIN_N:
                 continue
-            times = {t: time_plan(kind, n, t, samples) for t in variants(n)}
+            times = {t: time_plan(kind, n, t, samples) for t in variants(n, kind)}
             best = min(times, key=times.get)
             _lib.check(lib().fcb_tune_set(n, KINDS[kind], best))
             out[f"{kind}:{n}"] = {"threads": best, "ms": times}

@@ -47,7 +47,7 @@ def test_gpu_arm_line():
     env = dict(os.environ)
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "5", "--warmup", "3",
                         "--no-cpu-baseline", "--e2e-steps", "1", "--pulses", "64", "--batch-jobs", "8",
-                        "--serve-seconds", "2", "--serve-rate", "100"],
+                        "--serve-seconds", "2", "--serve-rate", "100", "--serve-check-every", "1"],
                        capture_output=True, text=True, env=env, timeout=900, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
