@@ -8,14 +8,13 @@ What it chooses (measured on the device with CUDA events, never guessed):
   samples, two per SM) or 512 threads (16384 samples, one per SM; rows of 4096
   samples and more), or 256 threads with 64 samples each (value -256, rows of
   16384 samples).  Rows longer than one CTA's samples split over a
-  thread-block cluster.  For the fused fast convolution of 32768-sample rows
-  there is also -2, the split variant: one 256-thread CTA per row runs the
-  row as two 16384-sample halves (64 samples per thread), holding the waiting
-  half in tensor memory.  The choice is installed with fcb_tune_set and
-  applies to plans made afterwards.
-* For the batched launch: the same CTA size (which also fixes the cluster
-  shape: 4 x 256 or 2 x 512 threads for 32768-sample rows) and the job order
-  (longest rows first, or as given).
+  thread-block cluster.  The choice is installed with fcb_tune_set and applies
+  to plans made afterwards.
+* For the batched launch: the kernel (CTAs of 256 or 512 threads with 32
+  samples each, clusters of 4 x 256 or 2 x 512 threads for 32768-sample rows;
+  or -256, the wide kernel: 256 threads with 64 samples each for rows of
+  16384 and 32768, clusters of 2 x 256 for 32768) and the job order (longest
+  rows first, or as given).
 
 The reference's analogue is FFTW's planning rigor chosen per Fftm object
 (src/ovxx/fftw/fft.cpp:44-52).  Results are cached as JSON keyed by GPU name,
@@ -33,19 +32,17 @@ KINDS = {"forward": 0, "inverse": 1, "fastconv": 2}
 VARIANT_MIN_N = 256  # below this every length has only the 256-thread kernel
 
 
-def variants(n: int, kind: str = "forward") -> tuple:
-    """Kernel variants the library has at row length n for `kind`: CTA sizes
-    with 32 samples per thread, -256 (256 threads x 64 samples) at 16384, and
-    -2 (two 64-sample halves, tensor memory) for the fused kind at 32768."""
+def variants(n: int) -> tuple:
+    """Kernel variants the library has at row length n: CTA sizes with 32
+    samples per thread, and -256 (256 threads x 64 samples) at 16384 and
+    32768 (a cluster of two such CTAs)."""
     out = [256]
     if 256 <= n <= 8192:
         out.insert(0, 128)
     if n >= 4096:
         out.append(512)
-    if n == 16384:
+    if n in (16384, 32768):
         out.append(-256)
-    if n == 32768 and kind == "fastconv":
-        out.append(-2)
     return tuple(out)
 
 
@@ -96,14 +93,14 @@ def tune_plans(lengths=(1024, 4096, 8192, 16384, 32768, 65536), kinds=tuple(KIND
         for n in lengths:
             if n < VARIANT_MIN_N:
                 continue
-            times = {t: time_plan(kind, n, t, samples) for t in variants(n, kind)}
+            times = {t: time_plan(kind, n, t, samples) for t in variants(n)}
             best = min(times, key=times.get)
             _lib.check(lib().fcb_tune_set(n, KINDS[kind], best))
             out[f"{kind}:{n}"] = {"threads": best, "ms": times}
     return out
 
 
-def tune_batch(make_batch, orders=("longest_first", "as_given"), threads=(256, 512), reps: int = 5) -> dict:
+def tune_batch(make_batch, orders=("longest_first", "as_given"), threads=(256, 512, -256), reps: int = 5) -> dict:
     """make_batch(threads, order) -> Batch with its jobs set; returns the best
     {"threads", "order", "ms"} and all timings."""
     results = {}

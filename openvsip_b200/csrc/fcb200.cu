@@ -118,42 +118,6 @@ __global__ void build_rep_kernel(const float2 *spec, long long spec_rs, float4 *
   rep[i] = make_float4(a.x * inv, b.x * inv, a.y * inv, b.y * inv);
 }
 
-// Replica tables of the split variant (rows of 2N run as two halves of N, see
-// rows_split_kernel): per row, the half schedule's table for the even bins
-// R[2m], then the one for the odd bins R[2m + 1], both scaled by 1/2N (exact
-// for powers of two).  s is the schedule of the half length N.
-__global__ void build_rep_split_kernel(const float2 *spec, long long spec_rs, float4 *rep, long long rows,
-                                       SchedRT s)
-{
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long total = rows * 2 * s.half;
-  if (i >= total) return;
-  long long r = i / (2 * s.half), e2 = i % (2 * s.half);
-  const long long part = e2 / s.half, e = e2 % s.half;
-  long long sigma = e;
-  if (s.ns > 1)
-  {
-    const long long tpr = s.n / s.ept, j = e / tpr, tr = e % tpr;
-    sigma = s.rb * tr + bitrev((int)j, s.lrb);
-  }
-  int qp = (int)(sigma / s.d), P = (int)(sigma % s.d);
-  int k = 2 * qp + s.r1 * digitrev16(P, s.ns - 1, s.lrb);  // bin pair (k, k + 1) of the half transform
-  const float inv = 0.5f / (float)s.n;
-  float2 a = spec[r * spec_rs + 2 * k + part], b = spec[r * spec_rs + 2 * (k + 1) + part];
-  rep[i] = make_float4(a.x * inv, b.x * inv, a.y * inv, b.y * inv);
-}
-
-// w[t] = exp(-2 pi i t / n2) for t < count, FP64 rounded once (the split
-// variant's per-thread W_2N^{tr}).
-__global__ void build_w2n_kernel(float2 *w, long long count, long long n2)
-{
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= count) return;
-  double sn, cs;
-  sincospi(-2.0 * (double)t / (double)n2, &sn, &cs);
-  w[t] = make_float2((float)cs, (float)sn);
-}
-
 // FP64 radix-2 Stockham FFT of one vector in global memory, one CTA.
 // Used once per replica (plan time), so simplicity beats speed here.
 __global__ void fft_fp64_kernel(const float2 *in, double2 *buf0, double2 *buf1, long long n,
@@ -294,28 +258,11 @@ static KernelInfo make_info()
 }
 
 
-template <int LOGN2>
-static KernelInfo make_split_info()
-{
-  using S = Sched<LOGN2 - 1, 256, 64>;
-  KernelInfo k;
-  k.fn = (const void *)&rows_split_kernel<LOGN2>;
-  k.ept = 64;
-  k.threads = 256;
-  k.cluster = 1;
-  k.rows_per_cta = 1;
-  k.smem = S::SMEM;
-  k.tw_bytes = S::tw_bytes() + 8LL * S::TPR;
-  k.split = 1;
-  return k;
-}
-
 template <int LOGN>
 static void fill_table(KernelInfo (*tab)[3][kVariants])
 {
   if constexpr (LOGN >= 1)
   {
-    if constexpr (LOGN == kSplitLog) tab[LOGN][kFastconv][4] = make_split_info<LOGN>();
     tab[LOGN][kFwd][0] = make_info<LOGN, kFwd, 256>();
     tab[LOGN][kInv][0] = make_info<LOGN, kInv, 256>();
     tab[LOGN][kFastconv][0] = make_info<LOGN, kFastconv, 256>();
@@ -331,7 +278,7 @@ static void fill_table(KernelInfo (*tab)[3][kVariants])
       tab[LOGN][kInv][2] = make_info<LOGN, kInv, 128>();
       tab[LOGN][kFastconv][2] = make_info<LOGN, kFastconv, 128>();
     }
-    if constexpr (LOGN == kWideLog)
+    if constexpr (LOGN >= kWideLog && LOGN <= kWideMaxLog)
     {
       tab[LOGN][kFwd][3] = make_info<LOGN, kFwd, 256, 64>();
       tab[LOGN][kInv][3] = make_info<LOGN, kInv, 256, 64>();
@@ -373,21 +320,20 @@ const KernelInfo *kernel_info(int logn, int mode)
 
 // Public tuning values: 128, 256, 512 threads (32 samples per thread), or -256
 // for the wide variant (256 threads x 64 samples).
-static int variant_id(int logn, int mode, int threads)
+static int variant_id(int logn, int threads)
 {
-  if (threads == -2 && logn == kSplitLog && mode == kFastconv) return 4;
-  if (threads == -256 && logn == kWideLog) return 3;
+  if (threads == -256 && logn >= kWideLog && logn <= kWideMaxLog) return 3;
   if (threads == 512 && logn >= kMin512) return 1;
   if (threads == 128 && logn >= kMin128 && logn <= kMax128) return 2;
   return threads == 256 ? 0 : -1;
 }
-static const int kVariantValue[kVariants] = {256, 512, 128, -256, -2};
+static const int kVariantValue[kVariants] = {256, 512, 128, -256};
 
 const KernelInfo *kernel_variant(int logn, int mode, int threads)
 {
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2) return nullptr;
-  const int v = variant_id(logn, mode, threads);
+  const int v = variant_id(logn, threads);
   return &g_table[logn][mode][v < 0 ? 0 : v];
 }
 
@@ -396,12 +342,12 @@ int set_variant(int logn, int mode, int threads)
   init_table();
   if (logn < 1 || logn > kMaxLogN || mode < 0 || mode > 2)
     return set_error(FCB_ERR_INVALID, "bad length or mode for tuning");
-  if (threads != 128 && threads != 256 && threads != 512 && threads != -256 && threads != -2)
-    return set_error(FCB_ERR_INVALID, "threads must be 128, 256, 512, -256 (wide) or -2 (split)");
-  const int v = variant_id(logn, mode, threads);
+  if (threads != 128 && threads != 256 && threads != 512 && threads != -256)
+    return set_error(FCB_ERR_INVALID, "threads must be 128, 256, 512 or -256 (wide)");
+  const int v = variant_id(logn, threads);
   if (v < 0)
     return set_error(FCB_ERR_UNSUPPORTED, "no %d-thread variant for rows of %d samples (512: 4096 and more; "
-                     "128: 256 .. 8192; -256: 16384; -2: fused rows of 32768)", threads, 1 << logn);
+                     "128: 256 .. 8192; -256: 16384 and 32768)", threads, 1 << logn);
   std::lock_guard<std::mutex> lk(g_variant_mu);
   g_variant[logn][mode] = v;
   return FCB_OK;
@@ -458,20 +404,15 @@ int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaSt
   return FCB_OK;
 }
 
-int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st, int split)
+int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st)
 {
-  // split: the half length's tables, then W_2N^t for t below the threads per row
-  SchedRT s = sched_rt(split ? logn - 1 : logn, ept);
-  const long long w2n = split ? (long long)s.n / ept : 0;
+  SchedRT s = sched_rt(logn, ept);
   float4 *tw = nullptr;
-  const size_t bytes = 16 * (size_t)s.half + 8 * (size_t)s.tw2_size + 8 * (size_t)w2n;
+  const size_t bytes = 16 * (size_t)s.half + 8 * (size_t)s.tw2_size;
   cudaError_t e = cudaMalloc(&tw, bytes);
   if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "twiddle table: %s", cudaGetErrorString(e));
   const long long entries = s.half + s.tw2_size;
   build_tw_kernel<<<(unsigned)((entries + 255) / 256), 256, 0, st>>>(tw, s);
-  if (split)
-    build_w2n_kernel<<<(unsigned)((w2n + 255) / 256), 256, 0, st>>>(
-        reinterpret_cast<float2 *>(reinterpret_cast<char *>(tw) + 16 * s.half + 8 * s.tw2_size), w2n, 2LL * s.n);
   e = cudaGetLastError();
   if (e != cudaSuccess) { cudaFree(tw); return cuda_error(e, "twiddle build"); }
   *out = tw;
@@ -479,17 +420,8 @@ int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st, int split)
 }
 
 int build_replica_table(int logn, int ept, const float2 *spec_dev, long long spec_rs, long long rows,
-                        float4 *rep_dev, cudaStream_t st, int split)
+                        float4 *rep_dev, cudaStream_t st)
 {
-  if (split)
-  {
-    SchedRT s = sched_rt(logn - 1, ept);
-    long long total = rows * 2 * s.half;
-    build_rep_split_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(spec_dev, spec_rs, rep_dev, rows, s);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_error(e, "replica table build");
-    return FCB_OK;
-  }
   SchedRT s = sched_rt(logn, ept);
   long long total = rows * s.half;
   build_rep_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(spec_dev, spec_rs, rep_dev, rows, s);

@@ -168,12 +168,7 @@ void plan_free(fcb_plan p)
   delete p;
 }
 
-int plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long long replica_rows,
-                  long long replica_rs, int replica_kind, int where, fcb_plan *plan, bool allow_split);
-
-// allow_split = false keeps the plan off the split variant (the Bluestein inner
-// plans, whose tables the chirp kernels read in the unsplit layout).
-int plan_common(fcb_plan p, long long n, long long rows_max, int mode, bool allow_split = true)
+int plan_common(fcb_plan p, long long n, long long rows_max, int mode)
 {
   int rc = check_device();
   if (rc) return rc;
@@ -188,10 +183,9 @@ int plan_common(fcb_plan p, long long n, long long rows_max, int mode, bool allo
   if (p->logn >= 1)
   {
     p->k = kernel_info(p->logn, mode);
-    if (p->k->split && !allow_split) p->k = kernel_variant(p->logn, mode, 512);
     rc = prepare_kernel(p->k);
     if (rc) return rc;
-    rc = build_twiddles(p->logn, p->k->ept, &p->tw, p->stream, p->k->split);
+    rc = build_twiddles(p->logn, p->k->ept, &p->tw, p->stream);
     if (rc) return rc;
   }
   return FCB_OK;
@@ -221,8 +215,8 @@ int blue_setup(fcb_plan p, long long n, long long rows_max, int mode, bool need_
     float2 *spec = nullptr;
     rc = bluestein_tables(n, m, d == 0 ? -1 : +1, &p->chirp[d], &spec, p->stream);
     if (rc) return rc;
-    rc = plan_fastconv(m, 1, reinterpret_cast<const fcb_cf32 *>(spec), 1, m, FCB_REPLICA_SPECTRUM, FCB_DEVICE,
-                       &p->inner[d], false);
+    rc = fcb_plan_fastconv(m, 1, reinterpret_cast<const fcb_cf32 *>(spec), 1, m, FCB_REPLICA_SPECTRUM, FCB_DEVICE,
+                           &p->inner[d]);
     cudaFree(spec);
     if (rc) return rc;
   }
@@ -716,16 +710,6 @@ int fcb_plan_fftm(long long n, long long rows_max, int exponent, float scale, fc
 int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long long replica_rows,
                       long long replica_rs, int replica_kind, int where, fcb_plan *plan)
 {
-  return plan_fastconv(n, rows_max, replica, replica_rows, replica_rs, replica_kind, where, plan, true);
-}
-
-}  // extern "C"
-
-namespace {
-
-int plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long long replica_rows,
-                  long long replica_rs, int replica_kind, int where, fcb_plan *plan, bool allow_split)
-{
   if (!plan) return set_error(FCB_ERR_INVALID, "plan pointer is NULL");
   *plan = nullptr;
   if (!fcb_supported_length(n))
@@ -739,8 +723,7 @@ int plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long
   fcb_plan p = new (std::nothrow) fcb_plan_s;
   if (!p) return set_error(FCB_ERR_NOMEM, "plan allocation");
   const bool blue = blue_length(n);
-  int rc = blue ? blue_setup(p, n, rows_max, kFastconv, true, true)
-               : plan_common(p, n, rows_max, kFastconv, allow_split);
+  int rc = blue ? blue_setup(p, n, rows_max, kFastconv, true, true) : plan_common(p, n, rows_max, kFastconv);
   float2 *spec = nullptr, *tmp = nullptr;
   if (!rc)
   {
@@ -780,7 +763,7 @@ int plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long
       if (!rc)
       {
         if (p->logn >= 1)
-          rc = build_replica_table(p->logn, p->k->ept, spec, n, replica_rows, p->rep, p->stream, p->k->split);
+          rc = build_replica_table(p->logn, p->k->ept, spec, n, replica_rows, p->rep, p->stream);
         else
         {
           // length 1: table entry (R.re, -, R.im, -)
@@ -807,10 +790,6 @@ int plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, long
   *plan = p;
   return FCB_OK;
 }
-
-}  // namespace
-
-extern "C" {
 
 int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, long long out_rs,
              long long rows, int where)

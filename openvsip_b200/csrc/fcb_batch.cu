@@ -6,13 +6,16 @@
 // Fftm -> vmmul -> Fftm sequence (benchmarks/fastconv.cpp:100-106), run one
 // after another on the host.
 //
-// Work decomposition: a job of P rows of N samples is cut into "units".  A unit
-// is the work of one hardware cluster of CSMAX CTAs for one step: CSMAX row
-// tiles when a row fits in one CTA, or CSMAX/CS rows when CS CTAs share a row.
-// Units of all jobs form one index space (jobs ordered longest rows first by
-// default); each cluster takes the next unit from a global ticket counter (the
-// only scratch memory, reset by a memset node of the same graph) until the
-// space is exhausted, so uneven jobs balance across the GPU.
+// Work decomposition: a job of P rows of N samples is cut into "units".  Jobs
+// whose rows span CS > 1 CTAs of a cluster come first: their unit is the work
+// of one hardware cluster of CSMAX CTAs for one step (CSMAX/CS rows).  The
+// other jobs' unit is one row tile of one CTA.  Each group of units forms one
+// index space (jobs ordered longest rows first by default); a cluster takes
+// the next cluster unit from a global ticket counter until those are gone,
+// then each of its CTAs takes single-CTA units from a second counter on its
+// own, so uneven jobs balance across the GPU and short rows never wait on a
+// cluster barrier.  The two counters are the only scratch memory, reset by a
+// memset node of the same graph.
 #include "fcb200.h"
 #include "fcb_engine.cuh"
 #include "fcb_internal.h"
@@ -44,81 +47,154 @@ __device__ __forceinline__ long long ld_cluster_s64(uint32_t addr)
   return v;
 }
 
-template <int T, int CSMAX>
-__global__ void __launch_bounds__(T, 512 / T)
-    batch_kernel(const BatchJob *__restrict__ jobs, int njobs, long long total_units, unsigned long long *ticket)
+// WIDE = 1: the wide kernel (T = 256, one CTA per SM): rows of 16384 and
+// 32768 samples run 64 samples per thread (the wide tile; 32768 on a cluster
+// of two CTAs), shorter rows 32 per thread.
+template <int L, int T, int WIDE>
+using BatchSched = Sched<L, T, (WIDE && L >= 14) ? 64 : 32>;
+
+// One unit of a job of rows of 2^logn samples: `r` is the CTA's place in the
+// unit (its cluster rank for units that span the cluster, 0 for units of one
+// CTA).  A unit is tiles_per_unit tiles; a tile of a row that spans CS CTAs is
+// run by the CS CTAs of ranks sub * CS .. sub * CS + CS - 1.
+template <int T, int CSMAX, int WIDE>
+__device__ __forceinline__ void run_unit(const RowArgs &A, int logn, long long lu, int tiles_per_unit, int r,
+                                         bool copy)
 {
-  __shared__ long long s_unit[2];
-  constexpr bool HC = CSMAX > 1;
-  const int hw_rank = HC ? (int)cg::this_cluster().block_rank() : 0;
-  int cur_logn = -1;
-#pragma unroll 1
-  for (int it = 0;; ++it)
+  switch (logn)
   {
-    // one ticket per cluster, broadcast from rank 0 (double-buffered by parity:
-    // slot it&1 is rewritten only after every CTA passed the next barrier)
-    if (hw_rank == 0 && threadIdx.x == 0) s_unit[it & 1] = (long long)atomicAdd(ticket, 1ULL);
-    long long u;
-    if constexpr (HC)
-    {
-      cluster_sync();
-      u = ld_cluster_s64(cluster_addr(smem_addr(&s_unit[it & 1]), 0));
-    }
-    else
-    {
-      __syncthreads();
-      u = s_unit[it & 1];
-    }
-    if (u >= total_units)
-    {
-      if constexpr (HC) cluster_sync();  // rank 0 stays until every CTA has read
-      break;
-    }
-    int lo = 0, hi = njobs - 1;
-    while (lo < hi)
-    {
-      const int mid = (lo + hi + 1) >> 1;
-      if (jobs[mid].unit_begin <= u) lo = mid; else hi = mid - 1;
-    }
-    const BatchJob &J = jobs[lo];
-    const long long lu = u - J.unit_begin;
-    const bool copy = J.logn != cur_logn;
-    cur_logn = J.logn;
-    switch (J.logn)
-    {
 #define FCB_BATCH_CASE(L)                                                                    \
   case L:                                                                                    \
   {                                                                                          \
-    constexpr int CS = Sched<L, T>::CS;                                                      \
+    using S = BatchSched<L, T, WIDE>;                                                        \
+    constexpr int CS = S::CS;                                                                \
     static_assert(CS <= CSMAX, "row longer than the launch's cluster");                      \
-    const int sub = hw_rank / CS;                                                            \
-    row_tile<L, kFastconv, T>(J.args, lu * J.tiles_per_unit + sub, hw_rank % CS, sub * CS, copy); \
+    const int sub = r / CS;                                                                  \
+    row_tile<L, kFastconv, T, (WIDE && L >= 14) ? 64 : 32>(A, lu * tiles_per_unit + sub, r % CS, sub * CS, copy); \
   }                                                                                          \
   break;
-      FCB_BATCH_CASE(8)
-      FCB_BATCH_CASE(9)
-      FCB_BATCH_CASE(10)
-      FCB_BATCH_CASE(11)
-      FCB_BATCH_CASE(12)
-      FCB_BATCH_CASE(13)
-      FCB_BATCH_CASE(14)
-      FCB_BATCH_CASE(15)
+    FCB_BATCH_CASE(8)
+    FCB_BATCH_CASE(9)
+    FCB_BATCH_CASE(10)
+    FCB_BATCH_CASE(11)
+    FCB_BATCH_CASE(12)
+    FCB_BATCH_CASE(13)
+    FCB_BATCH_CASE(14)
+    FCB_BATCH_CASE(15)
 #undef FCB_BATCH_CASE
-      default:
-        break;
+    default:
+      break;
+  }
+}
+
+// Persistent batch kernel.  Jobs [0, ncl) have rows that span several CTAs of
+// the cluster (units of the whole cluster, counted by ticket[0]); jobs
+// [ncl, njobs) have rows of one CTA (units of one CTA, ticket[1]).  A cluster
+// first takes cluster units, one ticket per cluster broadcast from rank 0, in
+// step; once they are gone each CTA takes single-CTA units on its own, with no
+// cluster barrier, so CTAs of a cluster do not wait on each other for short
+// rows.
+// Jobs whose first unit index is kept in shared memory for the lookup of a
+// unit's job (larger job lists are searched in global memory).
+constexpr int kSmemJobs = 1024;
+
+template <int T, int CSMAX, int WIDE = 0>
+__global__ void __launch_bounds__(T, WIDE ? 1 : 512 / T)
+    batch_kernel(const BatchJob *__restrict__ jobs, int ncl, int njobs, long long cl_units, long long solo_units,
+                 unsigned long long *ticket)
+{
+  __shared__ long long s_unit[2];
+  __shared__ long long s_begin[kSmemJobs];
+  // the current unit's job arguments: read from shared memory where they are
+  // used instead of being held in registers across the tile (fewer spills)
+  __shared__ RowArgs s_args;
+  constexpr bool HC = CSMAX > 1;
+  const int hw_rank = HC ? (int)cg::this_cluster().block_rank() : 0;
+  const bool smem_jobs = njobs <= kSmemJobs;
+  if (smem_jobs)
+    for (int i = threadIdx.x; i < njobs; i += T) s_begin[i] = jobs[i].unit_begin;
+  // (made visible by the first ticket barrier)
+  auto begin = [&](int i) { return smem_jobs ? s_begin[i] : jobs[i].unit_begin; };
+  int cur_logn = -1, cur_job = -1;
+  int it = 0;
+  bool cluster_phase = HC && cl_units > 0;
+  // Thread 0 (of rank 0 in the cluster phase) asks for the next unit while the
+  // current one runs, so the ticket's round trip is off the critical path.
+  long long next = 0;
+  if (threadIdx.x == 0 && (cluster_phase ? hw_rank == 0 : true))
+    next = (long long)atomicAdd(&ticket[cluster_phase ? 0 : 1], 1ULL);
+  // one loop and one call of the tile code (two inlined copies of it would
+  // not fit the wide kernel's registers)
+#pragma unroll 1
+  for (;; ++it)
+  {
+    long long u;
+    int first, last, r;
+    if (cluster_phase)
+    {
+      // double-buffered by parity: slot it&1 is rewritten only after every
+      // CTA of the cluster passed the next cluster barrier
+      if (hw_rank == 0 && threadIdx.x == 0) s_unit[it & 1] = next;
+      cluster_sync();
+      u = ld_cluster_s64(cluster_addr(smem_addr(&s_unit[it & 1]), 0));
+      if (u >= cl_units)
+      {
+        cluster_sync();  // rank 0 stays until every CTA has read
+        cluster_phase = false;
+        if (threadIdx.x == 0) next = (long long)atomicAdd(&ticket[1], 1ULL);
+        continue;
+      }
+      if (hw_rank == 0 && threadIdx.x == 0) next = (long long)atomicAdd(&ticket[0], 1ULL);
+      first = 0;
+      last = ncl - 1;
+      r = hw_rank;
     }
+    else
+    {
+      if (threadIdx.x == 0) s_unit[it & 1] = next;
+      __syncthreads();
+      u = s_unit[it & 1];
+      if (u >= solo_units) break;
+      if (threadIdx.x == 0) next = (long long)atomicAdd(&ticket[1], 1ULL);
+      first = ncl;
+      last = njobs - 1;
+      r = 0;
+    }
+    // the unit's job: a CTA's units only increase within a phase, so search
+    // from its current job on
+    int lo = cur_job >= first ? cur_job : first, hi = last;
+    while (lo < hi)
+    {
+      const int mid = (lo + hi + 1) >> 1;
+      if (begin(mid) <= u) lo = mid; else hi = mid - 1;
+    }
+    if (lo != cur_job)
+    {
+      // every thread of the CTA has left the previous tile (the ticket barrier above)
+      constexpr int W = sizeof(RowArgs) / 8;
+      static_assert(sizeof(RowArgs) % 8 == 0 && W <= T, "job arguments are copied as 8-byte words");
+      if (threadIdx.x < W)
+        reinterpret_cast<long long *>(&s_args)[threadIdx.x] =
+            reinterpret_cast<const long long *>(&jobs[lo].args)[threadIdx.x];
+      __syncthreads();
+      cur_job = lo;
+    }
+    const int logn = jobs[lo].logn;
+    const bool copy = logn != cur_logn;
+    cur_logn = logn;
+    run_unit<T, CSMAX, WIDE>(s_args, logn, u - begin(lo), jobs[lo].tiles_per_unit, r, copy);
   }
 }
 
 // Largest shared-memory footprint over the lengths a batch kernel handles.
-template <int T, int L = kBatchMinLog>
+template <int T, int WIDE = 0, int L = kBatchMinLog>
 constexpr int batch_smem()
 {
   if constexpr (L > kBatchMaxLog)
     return 0;
   else
   {
-    constexpr int a = Sched<L, T>::SMEM, b = batch_smem<T, L + 1>();
+    constexpr int a = BatchSched<L, T, WIDE>::SMEM, b = batch_smem<T, WIDE, L + 1>();
     return a > b ? a : b;
   }
 }
@@ -127,15 +203,19 @@ struct BatchVariant
 {
   const void *fn;
   int threads, csmax, smem;
+  int wide;  // 1: 64 samples per thread at 16384 and 32768 (their tables are built for that)
 };
 
 static BatchVariant batch_variant(int threads)
 {
+  using SW = BatchSched<kBatchMaxLog, 256, 1>;
+  if (threads == -256)
+    return {(const void *)&batch_kernel<256, SW::CS, 1>, 256, SW::CS, batch_smem<256, 1>(), 1};
   if (threads == 256)
     return {(const void *)&batch_kernel<256, Sched<kBatchMaxLog, 256>::CS>, 256, Sched<kBatchMaxLog, 256>::CS,
-            batch_smem<256>()};
+            batch_smem<256>(), 0};
   return {(const void *)&batch_kernel<512, Sched<kBatchMaxLog, 512>::CS>, 512, Sched<kBatchMaxLog, 512>::CS,
-          batch_smem<512>()};
+          batch_smem<512>(), 0};
 }
 
 }  // namespace fcb
@@ -158,6 +238,9 @@ struct fcb_batch_s
   BatchJob *h_jobs = nullptr;     // pinned staging for the job table
   bool direct = false;            // launch without a graph (job sets that change every run)
   int njobs = 0;
+  int ncl = 0;                    // jobs [0, ncl) have rows that span several CTAs
+  long long cl_units = 0;         // units of the whole cluster (ticket 0)
+  long long solo_units = 0;       // units of one CTA (ticket 1)
   long long total_units = 0;
   long long total_samples = 0;
   unsigned long long *d_ticket = nullptr;
@@ -217,10 +300,10 @@ int launch_batch(fcb_batch b, cudaStream_t st)
     cfg.numAttrs = 1;
   }
   const BatchJob *jobs = b->d_jobs;
-  int njobs = b->njobs;
-  long long total = b->total_units;
+  int ncl = b->ncl, njobs = b->njobs;
+  long long cl_units = b->cl_units, solo_units = b->solo_units;
   unsigned long long *ticket = b->d_ticket;
-  void *params[] = {&jobs, &njobs, &total, &ticket};
+  void *params[] = {&jobs, &ncl, &njobs, &cl_units, &solo_units, &ticket};
   cudaError_t e = cudaLaunchKernelExC(&cfg, b->v.fn, params);
   if (e != cudaSuccess) return cuda_error(e, "batch kernel launch");
   return FCB_OK;
@@ -232,7 +315,7 @@ int build_graph(fcb_batch b)
   drop_graph(b);
   cudaError_t e = cudaStreamBeginCapture(b->own_stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return cuda_error(e, "graph capture");
-  e = cudaMemsetAsync(b->d_ticket, 0, sizeof(unsigned long long), b->own_stream);
+  e = cudaMemsetAsync(b->d_ticket, 0, 2 * sizeof(unsigned long long), b->own_stream);
   int rc = e == cudaSuccess ? launch_batch(b, b->own_stream) : cuda_error(e, "ticket reset");
   cudaGraph_t g = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(b->own_stream, &g);
@@ -253,7 +336,8 @@ int fcb_batch_create(int threads, fcb_batch *out)
   if (!out) return set_error(FCB_ERR_INVALID, "batch pointer is NULL");
   *out = nullptr;
   if (threads == 0) threads = 512;
-  if (threads != 256 && threads != 512) return set_error(FCB_ERR_INVALID, "threads must be 0, 256 or 512");
+  if (threads != 256 && threads != 512 && threads != -256)
+    return set_error(FCB_ERR_INVALID, "threads must be 0, 256, 512 or -256 (wide)");
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return set_error(FCB_ERR_NODEVICE, "no CUDA device");
   fcb_batch b = new (std::nothrow) fcb_batch_s;
@@ -293,7 +377,7 @@ int fcb_batch_create(int threads, fcb_batch *out)
   if (!rc && (e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
     rc = cuda_error(e, "cudaStreamCreate");
   b->stream = b->own_stream;
-  if (!rc && (e = cudaMalloc(&b->d_ticket, sizeof(unsigned long long))) != cudaSuccess)
+  if (!rc && (e = cudaMalloc(&b->d_ticket, 2 * sizeof(unsigned long long))) != cudaSuccess)
     rc = set_error(FCB_ERR_NOMEM, "ticket counter: %s", cudaGetErrorString(e));
   if (rc) { batch_free(b); return rc; }
   *out = b;
@@ -326,9 +410,10 @@ int fcb_batch_add_replica(fcb_batch b, const fcb_cf32 *replica, long long n, int
   }
   if (!rc && (e = cudaMalloc(&table, sizeof(float4) * (size_t)(n / 2))) != cudaSuccess)
     rc = set_error(FCB_ERR_NOMEM, "replica table");
-  // the batch kernels run 32 samples per thread
-  if (!rc) rc = build_replica_table(l, 32, spec, n, 1, table, b->own_stream);
-  if (!rc && !b->tw[l]) rc = build_twiddles(l, 32, &b->tw[l], b->own_stream);
+  // the batch kernels run 32 samples per thread, the wide one 64 at 16384 and 32768
+  const int ept = (b->v.wide && l >= 14) ? 64 : 32;
+  if (!rc) rc = build_replica_table(l, ept, spec, n, 1, table, b->own_stream);
+  if (!rc && !b->tw[l]) rc = build_twiddles(l, ept, &b->tw[l], b->own_stream);
   if (!rc && (e = cudaStreamSynchronize(b->own_stream)) != cudaSuccess) rc = cuda_error(e, "replica preparation");
   cudaFree(spec);
   cudaFree(tmp);
@@ -358,7 +443,19 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) {
       return jobs[a].n != jobs[c].n ? jobs[a].n > jobs[c].n : jobs[a].pulses > jobs[c].pulses;
     });
-  long long units = 0, samples = 0;
+  // geometry of a length on the variant's CTAs (as in Sched<>): CTAs per row
+  auto ctas_per_row = [&](int l) {
+    const int ept = (b->v.wide && l >= 14) ? 64 : 32;
+    const int half = 1 << (l - 1), spc = b->v.threads * ept / 2;
+    return half > spc ? half / spc : 1;
+  };
+  // jobs whose rows span several CTAs first (units of the whole cluster),
+  // then the others (units of one CTA), each group in the chosen order
+  std::stable_partition(idx.begin(), idx.end(),
+                        [&](int i) { return ctas_per_row(b->replicas[jobs[i].replica].logn) > 1; });
+  long long units = 0, samples = 0, cl_units = 0;
+  int ncl = 0;
+  bool cluster_group = true;
   for (int i : idx)
   {
     const fcb_job &j = jobs[i];
@@ -366,13 +463,19 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     const int l = b->replicas[j.replica].logn;
     BatchJob bj = {};
     bj.logn = l;
-    // geometry of this length on the variant's CTAs (as in Sched<>)
     const int T = b->v.threads;
-    const int half = (int)(j.n / 2);
-    const int spc = T * 16;
-    const int cs = half > spc ? half / spc : 1;
-    const int rows_per_tile = cs > 1 ? 1 : (T * 32) / (int)j.n;
-    bj.tiles_per_unit = b->v.csmax / cs;
+    const int ept = (b->v.wide && l >= 14) ? 64 : 32;
+    const int cs = ctas_per_row(l);
+    if (cluster_group && cs == 1)
+    {
+      // the single-CTA group starts its own unit count
+      cluster_group = false;
+      cl_units = units;
+      units = 0;
+    }
+    if (cs > 1) ++ncl;
+    const int rows_per_tile = cs > 1 ? 1 : (T * ept) / (int)j.n;
+    bj.tiles_per_unit = cs > 1 ? b->v.csmax / cs : 1;
     const long long rows_per_unit = (long long)bj.tiles_per_unit * rows_per_tile;
     bj.unit_begin = units;
     units += (j.pulses + rows_per_unit - 1) / rows_per_unit;
@@ -390,15 +493,25 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     a.scale = 1.f;
     // L2 prefetch of the same job's rows about half a wave of units later
     // (units are taken in order; across a job boundary nothing is prefetched)
-    a.ahead = (long long)std::max(1, b->grid / b->v.csmax / 2) * bj.tiles_per_unit;
+    a.ahead = cs > 1 ? (long long)std::max(1, b->grid / b->v.csmax / 2) * bj.tiles_per_unit
+                     : (long long)std::max(1, b->grid / 2);
     hj.push_back(bj);
+  }
+  if (cluster_group)
+  {
+    // every job spans the cluster (or there are none)
+    cl_units = units;
+    units = 0;
   }
   cudaSetDevice(b->device);
   // the previous run of this batch may still read the job table
   cudaStreamSynchronize(b->stream);
   drop_graph(b);
   b->njobs = (int)hj.size();
-  b->total_units = units;
+  b->ncl = ncl;
+  b->cl_units = cl_units;
+  b->solo_units = units;
+  b->total_units = cl_units + units;
   b->total_samples = samples;
   b->direct = direct;
   if (hj.empty()) return FCB_OK;
@@ -433,7 +546,7 @@ int fcb_batch_run(fcb_batch b)
   cudaSetDevice(b->device);
   if (b->direct)
   {
-    cudaError_t e = cudaMemsetAsync(b->d_ticket, 0, sizeof(unsigned long long), b->stream);
+    cudaError_t e = cudaMemsetAsync(b->d_ticket, 0, 2 * sizeof(unsigned long long), b->stream);
     if (e != cudaSuccess) return cuda_error(e, "ticket reset");
     return launch_batch(b, b->stream);
   }

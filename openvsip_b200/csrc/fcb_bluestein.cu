@@ -123,7 +123,7 @@ static void fill_chirp(KernelInfo (*tab)[kVariants])
     tab[LOGN][0] = chirp_info<LOGN, 256>();
     if constexpr (LOGN >= kMin512) tab[LOGN][1] = chirp_info<LOGN, 512>();
     if constexpr (LOGN >= kMin128 && LOGN <= kMax128) tab[LOGN][2] = chirp_info<LOGN, 128>();
-    if constexpr (LOGN == kWideLog) tab[LOGN][3] = chirp_info<LOGN, 256, 64>();
+    if constexpr (LOGN >= kWideLog && LOGN <= kWideMaxLog) tab[LOGN][3] = chirp_info<LOGN, 256, 64>();
     fill_chirp<LOGN - 1>(tab);
   }
 }
@@ -136,7 +136,7 @@ const KernelInfo *chirp_kernel(int logn, const KernelInfo *like)
   std::call_once(g_chirp_once, [] { fill_chirp<kMaxLogN>(g_chirp); });
   if (logn < 3 || logn > kMaxLogN || !like) return nullptr;
   const int t = like->threads;
-  const int v = (like->ept == 64 && logn == kWideLog) ? 3
+  const int v = (like->ept == 64 && logn >= kWideLog && logn <= kWideMaxLog) ? 3
               : (t == 512 && logn >= kMin512) ? 1
               : (t == 128 && logn >= kMin128 && logn <= kMax128) ? 2 : 0;
   const KernelInfo *k = &g_chirp[logn][v];

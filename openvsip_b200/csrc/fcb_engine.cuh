@@ -166,27 +166,6 @@ __host__ __device__ constexpr float s64h(int k) { return k <= 16 ? cq64(16 - k) 
 __host__ __device__ constexpr float c64(int k) { return k < 32 ? c64h(k) : -c64h(k - 32); }
 __host__ __device__ constexpr float s64(int k) { return k < 32 ? s64h(k) : -s64h(k - 32); }
 
-// cos(2 pi k / 128) for k in [0, 32], correctly rounded to float.
-__host__ __device__ constexpr float cq128(int k)
-{
-  return k == 0 ? 1.0f : k == 1 ? 0.9987954497337341f : k == 2 ? 0.9951847195625305f : k == 3 ? 0.9891765117645264f
-       : k == 4 ? 0.9807852506637573f : k == 5 ? 0.9700312614440918f : k == 6 ? 0.9569403529167175f
-       : k == 7 ? 0.9415440559387207f : k == 8 ? 0.9238795042037964f : k == 9 ? 0.903989315032959f
-       : k == 10 ? 0.8819212913513184f : k == 11 ? 0.8577286005020142f : k == 12 ? 0.8314695954322815f
-       : k == 13 ? 0.803207516670227f : k == 14 ? 0.7730104327201843f : k == 15 ? 0.7409511208534241f
-       : k == 16 ? 0.7071067690849304f : k == 17 ? 0.6715589761734009f : k == 18 ? 0.6343932747840881f
-       : k == 19 ? 0.5956993103027344f : k == 20 ? 0.5555702447891235f : k == 21 ? 0.5141027569770813f
-       : k == 22 ? 0.4713967442512512f : k == 23 ? 0.4275550842285156f : k == 24 ? 0.3826834261417389f
-       : k == 25 ? 0.3368898630142212f : k == 26 ? 0.290284663438797f : k == 27 ? 0.24298018217086792f
-       : k == 28 ? 0.19509032368659973f : k == 29 ? 0.1467304676771164f : k == 30 ? 0.0980171412229538f
-       : k == 31 ? 0.049067676067352295f : 0.0f;
-}
-__host__ __device__ constexpr float c128h(int k) { return k <= 32 ? cq128(k) : -cq128(64 - k); }
-__host__ __device__ constexpr float s128h(int k) { return k <= 32 ? cq128(32 - k) : cq128(k - 32); }
-// cos and sin of 2 pi k / 128 for k in [0, 128).
-__host__ __device__ constexpr float c128(int k) { return k < 64 ? c128h(k) : -c128h(k - 64); }
-__host__ __device__ constexpr float s128(int k) { return k < 64 ? s128h(k) : -s128h(k - 64); }
-
 // Multiply a pair by the constant W_32^K = exp(SIGN * 2 pi i K / 32), 0 <= K < 16.
 template <int K, int SIGN>
 __device__ __forceinline__ cpair cp_rot32(cpair x)
@@ -484,19 +463,9 @@ __device__ __forceinline__ void half_wait()
 // while consecutive tiles have the same length).  The caller guarantees that
 // no thread of the CTA (or of the CS CTAs) still reads the slot array of a
 // previous tile.
-//
-// IO (optional): a policy object that replaces the tile's global I/O.  When
-// given, io->load<S>(a, row, tr, active, x) fills the stage-1 input x[j]
-// (sample tr + TPR j of the row) instead of the global loads and the L2
-// prefetch, and io->store_group<S>(a, row, tr, g, active, o) takes the
-// inverse stage-1 outputs of group g (o[k] is sample tr + TPR (g + G1 k),
-// k < R1) instead of the global stores.  Fused mode only.
-template <int LOGN, int MODE, int THREADS, int EPTW = 32, class IO = void>
-__device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int rank, int rank_base, bool copy_tw,
-                                         const IO *io = nullptr)
+template <int LOGN, int MODE, int THREADS, int EPTW = 32>
+__device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int rank, int rank_base, bool copy_tw)
 {
-  constexpr bool CUSTOM_IO = !std::is_void<IO>::value;
-  static_assert(!CUSTOM_IO || MODE == kFastconv, "custom I/O is for the fused mode");
   using S = Sched<LOGN, THREADS, EPTW>;
   constexpr int RB = S::RB, LRB = S::LRB;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
@@ -549,10 +518,6 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
   // ---------------- stage 1 (direction SIGN) ----------------
   {
     float2 x[S::EPT];
-    if constexpr (CUSTOM_IO)
-      io->template load<S>(a, row, tr, active, x);
-    else
-    {
     const float2 *src = a.in + row * a.in_rs;
     if constexpr (CHIRP)
     {
@@ -612,7 +577,6 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         }
       }
     }
-    }  // global loads
     // W_N^{tr q} for q = 2q' + lane; groups g > 0 add the constant W_32^{g q}
     float4 tw1[S::H1];
     if constexpr (S::NS > 1)
@@ -933,7 +897,6 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         for (int qp = 0; qp < S::H1; ++qp) z[qp] = c[g * S::H1 + bitrev(qp, LH1)];
       }
       DifNet<S::H1, +1>::run(z);  // z[i] = (A_r, B_r) with r = bitrev(i)
-      float2 o[CUSTOM_IO ? 2 * S::H1 : 1];
 #pragma unroll
       for (int i = 0; i < S::H1; ++i)
       {
@@ -945,12 +908,7 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
         if (k == 0) { tr_ = br; ti_ = bi; }
         else if (k == 8) { tr_ = -bi; ti_ = br; }
         else { tr_ = fmaf(br, wc, -bi * ws); ti_ = fmaf(br, ws, bi * wc); }
-        if constexpr (CUSTOM_IO)
-        {
-          o[r] = make_float2(ar + tr_, ai + ti_);
-          o[r + S::H1] = make_float2(ar - tr_, ai - ti_);
-        }
-        else if constexpr (CHIRP)
+        if constexpr (CHIRP)
         {
           // only the first n_out samples of the work row are wanted
           const int c0 = tr + S::TPR * g + S::D * r, c1 = c0 + S::D * S::H1;
@@ -967,7 +925,6 @@ __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int r
           dst_t[S::TPR * g + S::D * (r + S::H1)] = make_float2(ar - tr_, ai - ti_);
         }
       }
-      if constexpr (CUSTOM_IO) io->template store_group<S>(a, row, tr, g, active, o);
     }
     if constexpr (CL) cluster_sync_relaxed();
   }
@@ -982,209 +939,6 @@ __global__ void __launch_bounds__(THREADS, (Sched<LOGN, THREADS, EPTW>::MINB)) r
     row_tile<LOGN, MODE, THREADS, EPTW>(a, blockIdx.x / S::CS, (int)cg::this_cluster().block_rank(), 0, true);
   else
     row_tile<LOGN, MODE, THREADS, EPTW>(a, blockIdx.x, 0, 0, true);
-}
-
-
-// ---------------------------------------------------------------------------
-// Tensor memory (TMEM) as plain per-thread storage.  A warp reaches the 32
-// TMEM lanes of its quarter of the warpgroup (lanes 32 (warp % 4) ..); each
-// thread owns one lane, and an address is (lane << 16) | column, 32-bit
-// columns.  The CTA allocates TMEM with one warp and must free it before it
-// exits.
-__device__ __forceinline__ void tmem_alloc(uint32_t *smem_dst, uint32_t ncols)
-{
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-               :: "r"(smem_addr(smem_dst)), "r"(ncols) : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t ncols)
-{
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols) : "memory");
-}
-// Order TMEM accesses around a CTA barrier (before / after the bar.sync).
-__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
-
-// 32 consecutive columns of this thread's lane <- v (asynchronous store).
-__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32])
-{
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};"
-               :: "r"(taddr), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31]) : "memory");
-}
-// 16 consecutive columns of this thread's lane <- v (asynchronous store).
-__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16])
-{
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
-               :: "r"(taddr), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]) : "memory");
-}
-// v <- 32 consecutive columns of this thread's lane.  The wait names the
-// loaded registers as operands, so no use of them is scheduled before it.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
-{
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7]), "=f"(v[8]), "=f"(v[9]), "=f"(v[10]), "=f"(v[11]), "=f"(v[12]), "=f"(v[13]), "=f"(v[14]), "=f"(v[15]), "=f"(v[16]), "=f"(v[17]), "=f"(v[18]), "=f"(v[19]), "=f"(v[20]), "=f"(v[21]), "=f"(v[22]), "=f"(v[23]), "=f"(v[24]), "=f"(v[25]), "=f"(v[26]), "=f"(v[27]), "=f"(v[28]), "=f"(v[29]), "=f"(v[30]), "=f"(v[31]) : "r"(taddr) : "memory");
-  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]), "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]), "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]), "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]), "+f"(v[29]), "+f"(v[30]), "+f"(v[31]) :: "memory");
-}
-
-// ---------------------------------------------------------------------------
-// Rows of 2N samples on one CTA: the row is split into the two length-N
-// transforms of a radix-2 decimation in frequency, run one after the other by
-// the same row_tile schedule, with the half that waits held in tensor memory.
-//
-//   y0[n] = x[n] + x[n + N],  y1[n] = (x[n] - x[n + N]) W_2N^n    (n < N)
-//   FFT_N(y0)[m] = X[2m],     FFT_N(y1)[m] = X[2m + 1]
-//   z_p = IFFT_N(FFT_N(y_p) * R[2m + p] / 2N)  (unnormalised inverse)
-//   out[n] = z0[n] + W_2N^{-n} z1[n],  out[n + N] = z0[n] - W_2N^{-n} z1[n]
-//
-// Pass 0 (SplitIO<0>) loads x[n] and x[n + N] for the thread's samples, keeps y0 as the
-// stage-1 input and stores y1 in TMEM (region A); its inverse outputs z0 go to
-// TMEM too (region B).  Pass 1 (SplitIO<1>) reads y1 back, and its inverse outputs z1 are
-// combined with z0 and stored to global memory.  The row makes one HBM read
-// and one HBM write per sample with no cluster and no exchange between SMs.
-//
-// TMEM: 512 columns per CTA.  A thread's samples j < EPT (sample tr + TPR j)
-// sit as (re, im) at columns 32 g + 2 k for j = g + G1 k: region A at
-// columns [0, 128) of its warpgroup's 256, region B at [128, 256).
-template <int PASS>
-struct SplitIO
-{
-  uint32_t ta;   // TMEM address of this thread's warp lanes, its warpgroup's column 0
-  float2 wt;     // W_2N^{tr} = exp(-2 pi i tr / 2N)
-
-  template <class S>
-  __device__ __forceinline__ void load(const RowArgs &a, long long row, int tr, bool active,
-                                       float2 (&x)[S::EPT]) const
-  {
-    static_assert(S::CS == 1 && S::ROWS == 1 && S::EPT == 64 && S::R1 == 16 && 2 * S::N / S::TPR == 128,
-                  "the split schedule runs the wide 16384-sample tile");
-    constexpr int KG = S::R1;      // samples per stage-1 group (32 TMEM columns)
-    constexpr int KH = KG / 2;     // loaded and stored half a group at a time
-    if constexpr (PASS == 0)
-    {
-      const float2 *src = a.in + (active ? row : 0) * a.in_rs;
-#pragma unroll
-      for (int g = 0; g < S::G1; ++g)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-        {
-          float2 lo[KH], hi[KH];
-#pragma unroll
-          for (int k = 0; k < KH; ++k)
-          {
-            const int j = g + S::G1 * (h * KH + k);
-            lo[k] = active ? __ldg(src + tr + S::TPR * j) : make_float2(0.f, 0.f);
-            hi[k] = active ? __ldg(src + S::N + tr + S::TPR * j) : make_float2(0.f, 0.f);
-          }
-          float v[2 * KH];
-#pragma unroll
-          for (int k = 0; k < KH; ++k)
-          {
-            const int j = g + S::G1 * (h * KH + k);
-            x[j] = make_float2(lo[k].x + hi[k].x, lo[k].y + hi[k].y);
-            const float dr = lo[k].x - hi[k].x, di = lo[k].y - hi[k].y;
-            // W_2N^n = wt * W_128^j (n = tr + TPR j, 2N / TPR = 128), forward sign
-            const float cj = c128(j), sj = -s128(j);
-            const float wr = wt.x * cj - wt.y * sj, wi = wt.x * sj + wt.y * cj;
-            v[2 * k] = dr * wr - di * wi;
-            v[2 * k + 1] = dr * wi + di * wr;
-          }
-          tmem_st16(ta + 32u * g + 16u * h, v);
-        }
-      // the 2N-sample row `ahead` rows later streams into L2 while this one computes
-      if (a.ahead > 0 && row + a.ahead < a.rows)
-      {
-        constexpr int LINES = 2 * S::N / 16, PER = LINES / S::T;
-        const float2 *nxt = a.in + (row + a.ahead) * a.in_rs;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) prefetch_l2(nxt + 16 * (threadIdx.x + S::T * k));
-      }
-    }
-    else
-    {
-#pragma unroll
-      for (int g = 0; g < S::G1; ++g)
-      {
-        float v[2 * KG];
-        tmem_ld32(ta + 32u * g, v);
-#pragma unroll
-        for (int k = 0; k < KG; ++k) x[g + S::G1 * k] = make_float2(v[2 * k], v[2 * k + 1]);
-      }
-    }
-  }
-
-  template <class S>
-  __device__ __forceinline__ void store_group(const RowArgs &a, long long row, int tr, int g, bool active,
-                                              const float2 (&o)[2 * S::H1]) const
-  {
-    constexpr int KG = 2 * S::H1;
-    float v[2 * KG];
-    if constexpr (PASS == 0)
-    {
-#pragma unroll
-      for (int k = 0; k < KG; ++k) { v[2 * k] = o[k].x; v[2 * k + 1] = o[k].y; }
-      tmem_st32(ta + 128u + 32u * g, v);
-    }
-    else
-    {
-      tmem_ld32(ta + 128u + 32u * g, v);
-      float2 *dst = a.out + row * a.out_rs + tr;
-#pragma unroll
-      for (int k = 0; k < KG; ++k)
-      {
-        const int j = g + S::G1 * k;
-        // W_2N^{-n} = conj(wt) * W_128^{-j}
-        const float cj = c128(j), sj = s128(j);
-        const float wr = wt.x * cj + wt.y * sj, wi = wt.x * sj - wt.y * cj;
-        const float tr_ = o[k].x * wr - o[k].y * wi, ti_ = o[k].x * wi + o[k].y * wr;
-        if (active)
-        {
-          dst[S::TPR * j] = make_float2(v[2 * k] + tr_, v[2 * k + 1] + ti_);
-          dst[S::N + S::TPR * j] = make_float2(v[2 * k] - tr_, v[2 * k + 1] - ti_);
-        }
-      }
-    }
-  }
-};
-
-// The fused fast convolution of rows of 2^LOGN2 samples on one 256-thread CTA
-// per row, as two wide (64 samples per thread) transforms of half the length
-// with tensor memory holding the waiting half (SplitIO).  Tables: the half
-// length's twiddles, then W_2N^t for t < 256 (float2) after them; the replica
-// table holds the even-bin half's table, then the odd-bin half's, each scaled
-// by 1/2N.
-template <int LOGN2>
-__global__ void __launch_bounds__(256, 1) rows_split_kernel(RowArgs a)
-{
-  using S = Sched<LOGN2 - 1, 256, 64>;
-  static_assert(S::T == S::TPR, "one row per CTA");
-  __shared__ uint32_t s_tmem;
-  const int warp = threadIdx.x >> 5;
-  if (warp == 0) tmem_alloc(&s_tmem, 512);
-  tmem_fence_before();
-  __syncthreads();
-  tmem_fence_after();
-  const uint32_t tbase = s_tmem;
-  const uint32_t ta = tbase + ((32u * (warp & 3)) << 16) + 256u * (warp >> 2);
-  const float2 wt = reinterpret_cast<const float2 *>(reinterpret_cast<const char *>(a.tw) + S::tw_bytes())[threadIdx.x];
-  {
-    const SplitIO<0> io{ta, wt};
-    row_tile<LOGN2 - 1, kFastconv, 256, 64, SplitIO<0>>(a, blockIdx.x, 0, 0, true, &io);
-  }
-  tmem_wait_st();   // this thread's y1 and z0 are in TMEM before pass 1 reads them
-  __syncthreads();  // the second half reuses the slot array
-  {
-    RowArgs a1 = a;
-    a1.rep = a.rep + S::HALF;  // the odd-bin table
-    const SplitIO<1> io{ta, wt};
-    row_tile<LOGN2 - 1, kFastconv, 256, 64, SplitIO<1>>(a1, blockIdx.x, 0, 0, false, &io);
-  }
-  // every TMEM access of the CTA is complete before warp 0 frees the columns
-  tmem_wait_st();
-  tmem_fence_before();
-  __syncthreads();
-  tmem_fence_after();
-  if (warp == 0) tmem_free(tbase, 512);
 }
 
 }  // namespace fcb

@@ -26,17 +26,15 @@ struct KernelInfo
   long long tw_bytes = 0; // twiddle table size
   int ept = 32;          // samples per thread (the tables depend on it)
   long long resident_tiles = 0;  // CTAs (or clusters) resident at once, set by prepare_kernel
-  int split = 0;         // 1: rows of n run as two halves of n/2 on one CTA with the waiting half in
-                         // tensor memory (rows_split_kernel); tables are built for n/2
 };
 
 constexpr int kMin512 = 12;  // 512-thread variants exist for rows of 4096 samples and more
 constexpr int kMin128 = 8, kMax128 = 13;  // 128-thread variants: rows of 256 .. 8192 samples
-constexpr int kWideLog = 14;  // the wide variant (256 threads x 64 samples): rows of 16384 samples
-constexpr int kSplitLog = 15; // the split variant (two wide halves, tensor memory): fused rows of 32768
+constexpr int kWideLog = 14;     // the wide variant (256 threads x 64 samples): rows of 16384 samples,
+constexpr int kWideMaxLog = 15;  // and 32768 on clusters of two CTAs
 // Variant ids: [0] 256, [1] 512, [2] 128 threads with 32 samples each, [3] the
-// wide one, [4] the split one.  Their public tuning values are -256 and -2.
-constexpr int kVariants = 5;
+// wide one.  Its public tuning value is -256.
+constexpr int kVariants = 4;
 
 const KernelInfo *kernel_info(int logn, int mode);
 // Fused kernel with element-wise multipliers (kChirpconv, fcb_bluestein.cu)
@@ -49,10 +47,9 @@ int get_variant(int logn, int mode);
 int prepare_kernel(const KernelInfo *k);
 int launch_rows(const KernelInfo *k, long long rows, const RowArgs &args, cudaStream_t st);
 
-// split = 1: the tables of a split-variant kernel for rows of 2^logn (see KernelInfo::split)
-int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st, int split = 0);
+int build_twiddles(int logn, int ept, float4 **out, cudaStream_t st);
 int build_replica_table(int logn, int ept, const float2 *spec_dev, long long spec_rs, long long rows,
-                        float4 *rep_dev, cudaStream_t st, int split = 0);
+                        float4 *rep_dev, cudaStream_t st);
 int replica_spectrum_dev(const float2 *rep_dev, long long n, int matched, float2 *spec_dev,
                          cudaStream_t st);
 int launch_vmmul(const float2 *v, const float2 *m, long long m_rs, float2 *out, long long out_rs,

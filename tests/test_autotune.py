@@ -13,9 +13,7 @@ def test_variants_per_length():
     assert autotune.variants(4096) == (128, 256, 512)
     assert autotune.variants(8192) == (128, 256, 512)
     assert autotune.variants(16384) == (256, 512, -256)
-    assert autotune.variants(32768) == (256, 512)
-    assert autotune.variants(32768, "fastconv") == (256, 512, -2)
-    assert autotune.variants(16384, "fastconv") == (256, 512, -256)
+    assert autotune.variants(32768) == (256, 512, -256)
 
 
 @pytest.mark.gpu
@@ -26,8 +24,8 @@ def test_tune_installs_choice_and_cache_round_trip(tmp_path, monkeypatch):
     res = autotune.tune_plans(lengths=(1024, 16384), kinds=("fastconv",), samples=1 << 22)
     for n in (1024, 16384):
         r = res[f"fastconv:{n}"]
-        assert r["threads"] in autotune.variants(n, "fastconv")
-        assert set(r["ms"]) == set(autotune.variants(n, "fastconv")) and all(v > 0 for v in r["ms"].values())
+        assert r["threads"] in autotune.variants(n)
+        assert set(r["ms"]) == set(autotune.variants(n)) and all(v > 0 for v in r["ms"].values())
         assert lib.fcb_tune_get(n, autotune.KINDS["fastconv"]) == r["threads"]
     path = autotune.save(res)
     assert "fastconv:1024" in next(iter(json.load(open(path)).values()))

@@ -17,7 +17,7 @@ def _mix(seed, njobs, pulses=(16, 64), sizes=(256, 1024, 2048, 4096, 8192, 16384
     return synth.uneven_jobs(seed=seed, njobs=njobs, pulses=pulses, sizes=sizes)
 
 
-@pytest.mark.parametrize("threads", [256, 512])
+@pytest.mark.parametrize("threads", [256, 512, -256])
 def test_batch_uneven_jobs_vs_fp64(oracle, threads):
     import torch
     jobs = _mix(1, 20)
@@ -51,18 +51,26 @@ def test_batch_uneven_jobs_vs_fp64(oracle, threads):
         np.testing.assert_array_equal(y.cpu().numpy(), y0)
 
 
-def test_batch_equals_single_job_path_and_order(oracle):
+# single-job variants with the same arithmetic as each batch kernel: the
+# 256- and 512-thread kernels run 32 samples per thread at every length; the
+# wide one runs 64 at 16384 and 32768
+_SAME_ARITHMETIC = {512: {16384: 512, 32768: 512}, -256: {16384: -256, 32768: -256}}
+
+
+@pytest.mark.parametrize("threads", [512, -256])
+def test_batch_equals_single_job_path_and_order(oracle, threads):
     import torch
     jobs = _mix(2, 12, pulses=(3, 40))
-    b = Batch()
+    b = Batch(threads)
     jl, singles = [], []
+    pins = _SAME_ARITHMETIC[threads]
     for j in jobs:
         x = synth.job_data(j)
         rep = crandn(np.random.default_rng(j["seed"]), (j["n"],))
         rid = b.add_replica(rep, kind="spectrum")
         dx = torch.from_numpy(x).cuda()
         jl.append((dx, torch.empty_like(dx), rid))
-        with pinned_variant(16384, 2, 512):  # the batch kernels' arithmetic (32 samples per thread)
+        with pinned_variant(16384, 2, pins[16384]), pinned_variant(32768, 2, pins[32768]):
             singles.append(Fastconv(rep, x.shape[0])(dx))
     b.set_jobs(jl, order="as_given")
     b.run()
@@ -91,7 +99,8 @@ def test_batch_rejects_bad_jobs():
         b.add_replica(np.ones(65536, dtype=np.complex64))  # beyond the batch's 32768
 
 
-def test_c3_full_config_every_job_vs_fp64(oracle):
+@pytest.mark.parametrize("threads", [-256, 512])
+def test_c3_full_config_every_job_vs_fp64(oracle, threads):
     """The full uneven batch: 512 jobs, pulses U{16..512}, samples from
     {1024..32768}, each job with its own LFM replica (TBP U[50, 1000]), about
     1.45 G samples in one persistent launch.  Every job is checked against the
@@ -100,7 +109,7 @@ def test_c3_full_config_every_job_vs_fp64(oracle):
     import torch
     jobs = synth.uneven_jobs(seed=3, njobs=512)
     gen = torch.Generator(device="cuda")
-    b = Batch()
+    b = Batch(threads)
     xs, ys, chirps, jl = [], [], [], []
     for j in jobs:
         gen.manual_seed(int(j["seed"]))

@@ -15,7 +15,8 @@ RTOL = 2e-6
 
 
 @pytest.mark.parametrize("n,rows,threads", [(4096, 5, 512), (4096, 7, 512), (8192, 3, 512), (16384, 3, 512),
-                                            (16384, 1, -256), (16384, 3, -256), (32768, 3, 512)])
+                                            (16384, 1, -256), (16384, 3, -256), (32768, 3, 512), (32768, 1, -256),
+                                            (32768, 3, -256)])
 def test_staggered_variants_with_idle_rows(oracle, n, rows, threads):
     rng = np.random.default_rng(n + rows + threads)
     x = crandn(rng, (rows, n))
