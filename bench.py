@@ -388,7 +388,10 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
         bt.set_jobs([(x, y, i) for x, y, i in zip(xs, ys, ids)], order=order)
         return bt
 
-    tune = autotune.tune_batch(make, reps=3)
+    if args.batch_threads:
+        tune = {"threads": args.batch_threads, "order": "longest_first", "fixed": True}
+    else:
+        tune = autotune.tune_batch(make, reps=3)
     bt = make(tune["threads"], tune["order"])
     stream = torch.cuda.current_stream()
     bt.set_stream(stream.cuda_stream)
@@ -612,6 +615,8 @@ def main():
     ap.add_argument("--sweep", action="store_true", help="per-length throughput lines instead of the benchmark")
     ap.add_argument("--batch", action="store_true", help="uneven batched workload line instead of the benchmark")
     ap.add_argument("--batch-jobs", type=int, default=512)
+    ap.add_argument("--batch-threads", type=int, default=0,
+                    help="batch kernel variant (256, 512 or -256) instead of the autotuned one")
     ap.add_argument("--serve", action="store_true", help="served-stream line instead of the benchmark")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-seconds", type=float, default=60.0)
