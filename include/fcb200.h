@@ -157,10 +157,23 @@ FCB_API int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *r
 FCB_API int fcb_exec(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out,
              long long out_rs, long long rows, int where);
 
+/* fcb_exec without waiting: with where = FCB_HOST it queues the copies in,
+ * the kernels and the copies out of `rows` rows (chunked through the plan's
+ * device staging buffers) and returns; the caller keeps both host buffers
+ * untouched until fcb_sync returns.  Calls queued back to back on one plan run
+ * in order and overlap: the next call's copies in run while the previous
+ * call's last copies out drain (a streaming caller keeps the PCIe link busy in
+ * both directions across calls).  Host buffers should be pinned.  2-D plans
+ * run host calls synchronously.  No reference counterpart (the reference's
+ * Fftm calls are synchronous).  With where = FCB_DEVICE it is fcb_exec. */
+FCB_API int fcb_exec_async(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out,
+                           long long out_rs, long long rows, int where);
+
 /* Queue the plan's device work on a caller-owned cudaStream_t (NULL is the
  * CUDA default stream).  A new plan uses a private non-blocking stream. */
 FCB_API int fcb_set_stream(fcb_plan plan, void *stream);
-/* Wait for all work queued on the plan's stream. */
+/* Wait for all work queued on the plan's stream and, after host calls, its
+ * copy streams. */
 FCB_API int fcb_sync(fcb_plan plan);
 FCB_API int fcb_destroy(fcb_plan plan);
 

@@ -64,6 +64,7 @@ SIGNATURES = {
     "fcb_plan_fastconv": (c_int, [c_ll, c_ll, c_vp, c_ll, c_ll, c_int, c_int, ctypes.POINTER(c_vp)]),
     "fcb_plan_fft2d": (c_int, [c_ll, c_ll, c_int, c_float, ctypes.POINTER(c_vp)]),
     "fcb_exec": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_int]),
+    "fcb_exec_async": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_int]),
     "fcb_supported_real_length": (c_int, [c_ll]),
     "fcb_plan_fftm_real": (c_int, [c_ll, c_ll, c_int, c_float, ctypes.POINTER(c_vp)]),
     "fcb_exec_r2c": (c_int, [c_vp, c_vp, c_ll, c_vp, c_ll, c_ll, c_int]),

@@ -584,8 +584,9 @@ int ensure_staging(fcb_plan p, long long chunk_rows, int depth)
 // Copies in run on cin, kernels on the plan stream, copies out on cout, linked
 // by events, so both copy directions and the kernels overlap and the PCIe link
 // stays busy in both directions; a buffer is refilled once its copy out is done.
+// sync = false (fcb_exec_async): return once everything is queued.
 int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
-              long long rows)
+              long long rows, bool sync = true)
 {
   const size_t row_bytes = sizeof(float2) * (size_t)p->n;
   long long chunk = std::max<long long>(1, stage_bytes() / (long long)row_bytes);
@@ -625,7 +626,10 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
     const int b = (int)(c % depth);
     const long long nr = sizes[c];
     float2 *buf = p->stage[b];
-    if ((int)c >= depth) cudaStreamWaitEvent(p->cin, p->ev_out[b], 0);  // buffer drained
+    // buffer drained: by this call's copy out of chunk c - depth, or by the last
+    // copy out from it of an earlier call still in flight (asynchronous calls);
+    // an event never recorded is no wait
+    cudaStreamWaitEvent(p->cin, p->ev_out[b], 0);
     // dense rows move as one linear copy, strided rows as a pitched one
     cudaError_t e = in_rs == p->n
                       ? cudaMemcpyAsync(buf, in + r0 * in_rs, row_bytes * (size_t)nr, cudaMemcpyHostToDevice, p->cin)
@@ -644,6 +648,11 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
                               (size_t)nr, cudaMemcpyDeviceToHost, p->cout);
     if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "fcb_exec (host)");
     cudaEventRecord(p->ev_out[b], p->cout);
+  }
+  if (!sync)
+  {
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? FCB_OK : cuda_error(e, "fcb_exec_async (host)");
   }
   return host_done(p, FCB_OK, "fcb_exec (host)");
 }
@@ -791,8 +800,25 @@ int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *replica, 
   return FCB_OK;
 }
 
+int exec_impl(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, long long out_rs, long long rows,
+              int where, bool sync);
+
 int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, long long out_rs,
              long long rows, int where)
+{
+  return exec_impl(p, in, in_rs, out, out_rs, rows, where, true);
+}
+
+int fcb_exec_async(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, long long out_rs,
+                   long long rows, int where)
+{
+  return exec_impl(p, in, in_rs, out, out_rs, rows, where, false);
+}
+
+}  // extern "C"
+
+int exec_impl(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, long long out_rs, long long rows,
+              int where, bool sync)
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
   if (p->real) return set_error(FCB_ERR_INVALID, "real-FFT plans run through fcb_exec_r2c / fcb_exec_c2r");
@@ -831,8 +857,10 @@ int fcb_exec(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, lon
     return host_done(p, FCB_OK, "fcb_exec (2-D, host)");
   }
   if (where == FCB_DEVICE) return exec_device(p, i2, in_rs, o2, out_rs, rows, 0, p->stream);
-  return exec_host(p, i2, in_rs, o2, out_rs, rows);
+  return exec_host(p, i2, in_rs, o2, out_rs, rows, sync);
 }
+
+extern "C" {
 
 int fcb_set_stream(fcb_plan p, void *stream)
 {
@@ -845,9 +873,7 @@ int fcb_sync(fcb_plan p)
 {
   if (!p) return set_error(FCB_ERR_INVALID, "plan is NULL");
   DeviceGuard g(p->device);
-  cudaError_t e = cudaStreamSynchronize(p->stream);
-  if (e != cudaSuccess) return cuda_error(e, "fcb_sync");
-  return FCB_OK;
+  return host_done(p, FCB_OK, "fcb_sync");
 }
 
 int fcb_destroy(fcb_plan p)

@@ -135,7 +135,7 @@ class _Plan:
         return {"n": n.value, "cluster_ctas": cl.value, "rows_per_cta": rpc.value, "smem_bytes": sm.value,
                 "threads": th.value}
 
-    def _exec(self, inp, out):
+    def _exec(self, inp, out, wait: bool = True):
         ip, r, c, irs, iw = _desc(inp, False)
         op, r2, c2, ors, ow = _desc(out, True)
         if (r, c) != (r2, c2):
@@ -146,8 +146,21 @@ class _Plan:
         if iw != ow:
             raise ValueError("input and output must both be host arrays or both device tensors")
         _bind_stream(self._handle, iw)
-        check(lib().fcb_exec(self._handle, ctypes.c_void_p(ip), irs, ctypes.c_void_p(op), ors, r, iw))
+        fn = lib().fcb_exec if wait else lib().fcb_exec_async
+        check(fn(self._handle, ctypes.c_void_p(ip), irs, ctypes.c_void_p(op), ors, r, iw))
         return out
+
+    def submit(self, inp, out):
+        """Queue ``plan(inp, out)`` and return at once (fcb_exec_async).  With
+        host arrays the copies in, the kernels and the copies out run in the
+        background, and calls submitted back to back overlap on the PCIe link;
+        both arrays (pinned host memory, e.g. from torch's pin_memory) must stay
+        untouched until sync().  With CUDA tensors it is the same as a call."""
+        return self._exec(inp, out, wait=False)
+
+    def sync(self) -> None:
+        """Wait for everything submitted to this plan."""
+        check(lib().fcb_sync(self._handle))
 
     def __call__(self, inp, out=None):
         """``plan(in, out)`` by reference, ``plan(inout)`` ... see subclasses."""

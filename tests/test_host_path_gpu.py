@@ -58,3 +58,29 @@ def test_host_calls_back_to_back_and_in_place():
     inplace = xs[0].copy()
     fc.in_place(inplace)
     np.testing.assert_array_equal(inplace, outs[0])
+
+
+@pytest.mark.parametrize("rows,n,steps", [(600, 16384, 4), (1000, 2048, 3), (50, 1000, 3)])
+def test_submitted_host_calls_equal_single_calls(oracle, rows, n, steps):
+    # calls queued back to back with submit() (fcb_exec_async) reuse the plan's
+    # staging buffers while earlier calls still drain: every step's output must
+    # equal its own synchronous call's, bit for bit (n = 1000: Bluestein rows)
+    import torch
+    rng = np.random.default_rng(rows * n + steps)
+    rep = crandn(rng, (n,))
+    fc = Fastconv(rep, rows)
+    xs = [torch.from_numpy(crandn(rng, (rows, n))).pin_memory().numpy() for _ in range(steps)]
+    ys = [torch.empty((rows, n), dtype=torch.complex64).pin_memory().numpy() for _ in range(steps)]
+    for x, y in zip(xs, ys):
+        fc.submit(x, y)
+    fc.sync()
+    for x, y in zip(xs, ys):
+        np.testing.assert_array_equal(y, fc(x))
+    r = rows // 3
+    assert oracle.rel_l2(ys[-1][r:r + 1], oracle.fastconv(xs[-1][r:r + 1], rep)) <= RTOL
+    # one output buffer reused by every step (the last step's result stays)
+    out = torch.empty((rows, n), dtype=torch.complex64).pin_memory().numpy()
+    for x in xs:
+        fc.submit(x, out)
+    fc.sync()
+    np.testing.assert_array_equal(out, fc(xs[-1]))
