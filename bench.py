@@ -366,7 +366,8 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
     from openvsip_b200 import autotune, shard, synth
     from openvsip_b200.batch import Batch
     from openvsip_b200.vsip import Fastconv
-    jobs = synth.uneven_jobs(seed=3, njobs=args.batch_jobs)
+    sizes = tuple(int(v) for v in args.batch_sizes.split(",")) if args.batch_sizes else synth.SIZES
+    jobs = synth.uneven_jobs(seed=3, njobs=args.batch_jobs, sizes=sizes)
     if world > 1:
         mine = shard.partition_jobs([(j["pulses"], j["n"]) for j in jobs], world)[rank]
     else:
@@ -430,7 +431,8 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
     srt = sorted(ms)
     max_err = shard.max_over_ranks(max(errs))
     return {
-        "workload": BATCH_WORKLOAD.format(jobs=len(jobs)), "samples_per_step": all_samples,
+        "workload": BATCH_WORKLOAD.format(jobs=len(jobs)) + (f" (row lengths {sizes} only)" if args.batch_sizes else ""),
+        "samples_per_step": all_samples,
         "value": all_samples / (mean / 1e3), "unit": "complex samples/s", "ms_per_step": mean, "steps": steps,
         "scaling": "strong" if world > 1 else None,
         "latency_ms": {"p50": srt[len(srt) // 2], "p99": srt[min(len(srt) - 1, int(0.99 * len(srt)))]},
@@ -615,6 +617,8 @@ def main():
     ap.add_argument("--sweep", action="store_true", help="per-length throughput lines instead of the benchmark")
     ap.add_argument("--batch", action="store_true", help="uneven batched workload line instead of the benchmark")
     ap.add_argument("--batch-jobs", type=int, default=512)
+    ap.add_argument("--batch-sizes", default="",
+                    help="comma-separated row lengths of the batch's jobs (profiling one length; default the mix)")
     ap.add_argument("--batch-threads", type=int, default=0,
                     help="batch kernel variant (256, 512 or -256) instead of the autotuned one")
     ap.add_argument("--serve", action="store_true", help="served-stream line instead of the benchmark")

@@ -491,10 +491,12 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     a.rep = b->replicas[j.replica].table;
     a.rep_rs = 0;
     a.scale = 1.f;
-    // L2 prefetch of the same job's rows about half a wave of units later
-    // (units are taken in order; across a job boundary nothing is prefetched)
-    a.ahead = cs > 1 ? (long long)std::max(1, b->grid / b->v.csmax / 2) * bj.tiles_per_unit
-                     : (long long)std::max(1, b->grid / 2);
+    // L2 prefetch of the same job's rows about a quarter of a wave of units
+    // later (units are taken in order; across a job boundary nothing is
+    // prefetched).  Measured on the 512-job mix: a quarter wave 0.321 of HBM,
+    // half a wave 0.319, a whole wave 0.316, none 0.309.
+    a.ahead = cs > 1 ? (long long)std::max(1, b->grid / b->v.csmax / 4) * bj.tiles_per_unit
+                     : (long long)std::max(1, b->grid / 4);
     hj.push_back(bj);
   }
   if (cluster_group)

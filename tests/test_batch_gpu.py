@@ -141,3 +141,32 @@ def test_c3_full_config_every_job_vs_fp64(oracle, threads):
         assert err <= RTOL, f"job {k} ({j['pulses']} x {j['n']}): rel-L2 {err:.3e}"
     # no job row was left unwritten (NaN-filled outputs)
     assert all(bool(torch.isfinite(torch.view_as_real(y)).all()) for y in ys)
+
+
+@pytest.mark.parametrize("threads", [512, -256])
+def test_batch_more_jobs_than_the_shared_index(oracle, threads):
+    # more than 1024 jobs: the unit -> job lookup runs on the job table in global
+    # memory instead of its copy in shared memory; every job equals the
+    # single-job path (the same arithmetic) and the first and last match FP64
+    import torch
+    rng = np.random.default_rng(1100)
+    b = Batch(threads)
+    n_list = [256, 512, 1024]
+    reps = {n: crandn(rng, (n,)) for n in n_list}
+    rids = {n: b.add_replica(reps[n], kind="spectrum") for n in n_list}
+    jl, xs = [], []
+    for k in range(1100):
+        n = n_list[k % 3]
+        x = crandn(rng, (1 + k % 3, n))
+        dx = torch.from_numpy(x).cuda()
+        jl.append((dx, torch.full_like(dx, float("nan")), rids[n]))
+        xs.append(x)
+    b.set_jobs(jl, order="as_given")
+    b.run()
+    b.sync()
+    plans = {n: Fastconv(reps[n], 3) for n in n_list}
+    for (dx, dy, _), x in zip(jl, xs):
+        np.testing.assert_array_equal(dy.cpu().numpy(), plans[x.shape[1]](dx).cpu().numpy())
+    for k in (0, 1099):
+        n = xs[k].shape[1]
+        assert oracle.rel_l2(jl[k][1].cpu().numpy(), oracle.fastconv(xs[k], reps[n])) <= RTOL
