@@ -281,10 +281,14 @@ def run_sweep(args):
     :100-106) and the forward row Fftm, on three shapes: the reference
     benchmark's 64 rows x 2^4 .. 2^16 (benchmarks/fastconv.cpp:977-988), the
     256 x {256 .. 65536} row sweep, and a fixed 2^24-sample batch per length;
-    then the 4096 x 4096 2-D FFT.  Kernel time by CUDA events."""
+    then the 4096 x 4096 2-D FFT.  Kernel time by CUDA events.  The Fftm and
+    2-D lines carry the forward transform's rel-L2 against FP64 (numpy) and the
+    forward -> inverse round trip's rel-L2 against the input, on uniform
+    [-1, 1] data."""
     import torch
 
     import openvsip_b200 as ov
+    from openvsip_b200 import synth
     torch.cuda.set_device(0)
     peak, _ = measured_peak()
     stream = torch.cuda.current_stream()
@@ -311,28 +315,45 @@ def run_sweep(args):
                 ov.vmmul(rep, tmp, tmp)
                 inv(tmp, y)
 
+            # accuracy on up to 8 rows of uniform [-1, 1] data: the forward transform against FP64,
+            # and the round trip forward -> inverse (scale 1/n) against the input
+            u = torch.from_numpy(synth.sweep_matrix(logn, min(rows, 8), n)).cuda()
+            fu = fwd(u)
+            back = inv(fu)
+            un = u.cpu().numpy()
+            acc = {"fwd_rel_l2_vs_fp64": rel_l2(fu.cpu().numpy(), np.fft.fft(un.astype(np.complex128), axis=1)),
+                   "roundtrip_rel_l2": rel_l2(back.cpu().numpy(), un)}
             for kind, fn, bps in (("fastconv", lambda: fc(x, y), 16.0), ("phased", phased, 48.0),
                                   ("fftm_fwd", lambda: fwd(x, y), 16.0)):
                 steps = args.steps if rows * n >= (1 << 20) else max(args.steps, 2000)
                 ms = _time_calls(fn, steps, stream)
                 alg = bps * rows * n + (8.0 * n if kind != "fftm_fwd" else 0.0)
                 gbs = alg / (ms / 1e3) / 1e9
-                print(json.dumps({"sweep": kind, "n": n, "rows": rows, "shape": label, "ms": ms,
-                                  "samples_per_s": rows * n / (ms / 1e3), "gbs": gbs, "frac": gbs / peak,
-                                  "alg_bytes_per_sample": bps, "l2_resident": 16 * rows * n < L2_BYTES,
-                                  "launches_per_call": 3 if kind == "phased" else 1,
-                                  "threads": fc.info()["threads"], "cluster": fc.info()["cluster_ctas"]}),
-                      flush=True)
+                line = {"sweep": kind, "n": n, "rows": rows, "shape": label, "ms": ms,
+                        "samples_per_s": rows * n / (ms / 1e3), "gbs": gbs, "frac": gbs / peak,
+                        "alg_bytes_per_sample": bps, "l2_resident": 16 * rows * n < L2_BYTES,
+                        "launches_per_call": 3 if kind == "phased" else 1,
+                        "threads": fc.info()["threads"], "cluster": fc.info()["cluster_ctas"]}
+                if kind == "fftm_fwd":
+                    line.update(acc)
+                print(json.dumps(line), flush=True)
             del fc, fwd, inv
-    # 4096 x 4096 2-D FFT, forward and inverse (two HBM passes each: 32 B/sample)
-    x = torch.randn(4096, 4096, dtype=torch.complex64, device="cuda")
+    # 4096 x 4096 2-D FFT, forward and inverse (two HBM passes each: 32 B/sample), uniform [-1, 1]
+    # data; round trip against the input and the forward transform against FP64
+    x = torch.from_numpy(synth.sweep_matrix(4096, 4096, 4096)).cuda()
     y = torch.empty_like(x)
-    for name, plan in (("fft2d_fwd", ov.Fft2d(4096, 4096, ov.fft_fwd)),
-                       ("fft2d_inv", ov.Fft2d(4096, 4096, ov.fft_inv, 1.0 / 4096 ** 2))):
+    f2, g2 = ov.Fft2d(4096, 4096, ov.fft_fwd), ov.Fft2d(4096, 4096, ov.fft_inv, 1.0 / 4096 ** 2)
+    X = f2(x)
+    xn = x.cpu().numpy()
+    acc = {"fwd_rel_l2_vs_fp64": rel_l2(X.cpu().numpy(), np.fft.fft2(xn.astype(np.complex128))),
+           "roundtrip_rel_l2": rel_l2(g2(X).cpu().numpy(), xn)}
+    del X
+    for name, plan in (("fft2d_fwd", f2), ("fft2d_inv", g2)):
         ms = _time_calls(lambda: plan(x, y), args.steps, stream)
         gbs = 32.0 * 4096 * 4096 / (ms / 1e3) / 1e9
         print(json.dumps({"sweep": name, "n": 4096, "rows": 4096, "shape": "4096 x 4096", "ms": ms,
-                          "samples_per_s": 4096 * 4096 / (ms / 1e3), "gbs": gbs, "frac": gbs / peak}), flush=True)
+                          "samples_per_s": 4096 * 4096 / (ms / 1e3), "gbs": gbs, "frac": gbs / peak, **acc}),
+              flush=True)
 
 
 def _cgauss_dev(rows, n, gen):
@@ -428,6 +449,20 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
     # the plain per-call GPU form: one fused launch per job, plans prepared beforehand
     plans = [Fastconv(c, x.shape[0], kind="matched") for c, x in zip(chirps, xs)]
     per_call_ms = shard.max_over_ranks(_time_calls(lambda: [p_(x, y) for p_, x, y in zip(plans, xs, ys)], 3, stream))
+    del plans
+    # and the phased Impl1op form per job (forward Fftm, vmmul<0>, inverse Fftm: three launches)
+    from openvsip_b200.vsip import Fftm, fft_fwd, fft_inv, replica_spectrum, vmmul
+    phased = [(Fftm(x.shape[0], x.shape[1], fft_fwd), Fftm(x.shape[0], x.shape[1], fft_inv, 1.0 / x.shape[1]),
+               replica_spectrum(torch.from_numpy(c).cuda(), matched=True)) for c, x in zip(chirps, xs)]
+
+    def run_phased():
+        for (f, g, spec), x, y in zip(phased, xs, ys):
+            f(x, y)
+            vmmul(spec, y, y)
+            g(y, y)
+
+    phased_ms = shard.max_over_ranks(_time_calls(run_phased, 3, stream))
+    del phased
     srt = sorted(ms)
     max_err = shard.max_over_ranks(max(errs))
     return {
@@ -444,7 +479,11 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
         "tuning": tune, "batch": bt.info(), "gpu_launches_per_step": 1,
         "per_call": {"ms": per_call_ms, "value": all_samples / (per_call_ms / 1e3), "launches_per_step": len(plans),
                      "how": "one fused Fastconv launch per job, plans prepared beforehand, device data"},
-        "batch_over_per_call": per_call_ms / mean, "clocks": clk.summary()}
+        "batch_over_per_call": per_call_ms / mean,
+        "per_call_phased": {"ms": phased_ms, "value": all_samples / (phased_ms / 1e3), "launches_per_step": 3 * len(xs),
+                            "how": "forward Fftm, vmmul<0>, inverse Fftm per job (the reference benchmark's Impl1op "
+                                   "form), plans prepared beforehand, device data"},
+        "batch_over_per_call_phased": phased_ms / mean, "clocks": clk.summary()}
 
 
 def run_batch(args):
@@ -596,11 +635,46 @@ def phased_block(ov, x, y, chirp_dev, pulses, nsamp, steps, stream) -> dict:
     ms = _time_calls(step, steps, stream)
     alg = 48.0 * pulses * nsamp + 8.0 * nsamp
     peak, _ = measured_peak()
+    # Impl1ip: the same three steps in place on one buffer (benchmarks/fastconv.cpp, the in-place form)
+    work = torch.empty_like(y)
+
+    def step_ip():
+        fwd(work, work)
+        ov.vmmul(spec, work, work)
+        inv(work, work)
+
+    work.copy_(x)
+    ms_ip = _time_calls(step_ip, steps, stream)
     return {"form": "Impl1op: Fftm(fwd) -> vmmul<0> -> Fftm(inv, 1/N), three launches per step",
             "value": pulses * nsamp / (ms / 1e3), "unit": "complex samples/s", "ms_per_step": ms, "steps": steps,
             "roofline": {"bound": "hbm", "alg_bytes_per_step": alg, "achieved": alg / (ms / 1e3) / 1e9,
                          "peak": peak, "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak},
-            "gpu_launches_per_step": 3}
+            "gpu_launches_per_step": 3,
+            "in_place": {"form": "Impl1ip: the same three launches in place on one buffer",
+                         "value": pulses * nsamp / (ms_ip / 1e3), "ms_per_step": ms_ip,
+                         "frac": alg / (ms_ip / 1e3) / 1e9 / peak}}
+
+
+def matrix_block(ov, x, y, chirp, pulses, nsamp, steps, stream) -> dict:
+    """The reference benchmark's matrix-of-coefficients form (Impl4mc,
+    benchmarks/fastconv.cpp:857-969): inv_fftm(W * fwd_fftm(x)) with one
+    replica spectrum per pulse, fused in one launch; the replica matrix is read
+    once per step, so the algorithmic traffic is 24 B per sample."""
+    import torch
+    w = np.conj(np.fft.fft(chirp.astype(np.complex128)))[None, :] * np.exp(
+        2j * np.pi * np.arange(pulses)[:, None] / pulses)          # a different spectrum per pulse
+    fc = ov.Fastconv(w.astype(np.complex64), pulses)
+    ms = _time_calls(lambda: fc(x, y), steps, stream)
+    alg = 24.0 * pulses * nsamp
+    peak, _ = measured_peak()
+    ys = y[:8].cpu().numpy()
+    ref = np.fft.ifft(np.fft.fft(x[:8].cpu().numpy().astype(np.complex128), axis=1) *
+                      w[:8].astype(np.complex64).astype(np.complex128), axis=1)
+    return {"form": "Impl4mc: inv_fftm(W * fwd_fftm(x)), one spectrum per pulse, one fused launch per step",
+            "value": pulses * nsamp / (ms / 1e3), "unit": "complex samples/s", "ms_per_step": ms, "steps": steps,
+            "roofline": {"bound": "hbm", "alg_bytes_per_step": alg, "achieved": alg / (ms / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak},
+            "rel_l2_vs_fp64": rel_l2(ys, ref), "gpu_launches_per_step": 1}
 
 
 def main():
@@ -725,6 +799,7 @@ def main():
     # the phased Impl1op form on the same device data
     phased = phased_block(ov, xin[0], yout, torch.from_numpy(chirp).cuda(), pulses, nsamp, min(args.steps, 50),
                           stream)
+    matrix = matrix_block(ov, xin[0], yout, chirp, pulses, nsamp, min(args.steps, 50), stream)
 
     # end to end through the public API with pinned host buffers: every step copies its input
     # in and its result out.  Streamed: the steps are submitted back to back (Fastconv.submit,
@@ -797,6 +872,7 @@ def main():
                                            "how": "Fastconv(host pinned in, host pinned out), each call waits "
                                                   "for its result"}},
             "phased": phased,
+            "matrix_of_coefficients": matrix,
             "batch": batch,
             "serve": serve,
             "gpu_launches": args.steps,

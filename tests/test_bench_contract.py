@@ -64,9 +64,13 @@ def test_gpu_arm_line():
     assert line["rel_l2_vs_fp64"] <= 2e-6
     ph = line["phased"]
     assert ph["value"] > 0 and ph["gpu_launches_per_step"] == 3 and ph["roofline"]["frac"] > 0
+    assert ph["in_place"]["value"] > 0
+    mc = line["matrix_of_coefficients"]
+    assert mc["value"] > 0 and mc["rel_l2_vs_fp64"] <= 2e-6
     b = line["batch"]
     assert b["value"] > 0 and b["rel_l2_vs_fp64"]["max"] <= 2e-6 and b["rel_l2_vs_fp64"]["jobs_checked"] == 8
     assert b["per_call"]["launches_per_step"] == 8 and b["batch_over_per_call"] > 0
+    assert b["per_call_phased"]["launches_per_step"] == 24 and b["batch_over_per_call_phased"] > 0
     sv = line["serve"]
     assert sv["jobs"] > 0 and sv["rel_l2_vs_fp64"]["jobs_checked"] == sv["jobs"]
     assert sv["rel_l2_vs_fp64"]["max"] <= 2e-6 and sv["latency_ms"]["p99"] >= sv["latency_ms"]["p50"] > 0
