@@ -449,6 +449,7 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
     # the plain per-call GPU form: one fused launch per job, plans prepared beforehand
     plans = [Fastconv(c, x.shape[0], kind="matched") for c, x in zip(chirps, xs)]
     per_call_ms = shard.max_over_ranks(_time_calls(lambda: [p_(x, y) for p_, x, y in zip(plans, xs, ys)], 3, stream))
+    n_plans = len(plans)
     del plans
     # and the phased Impl1op form per job (forward Fftm, vmmul<0>, inverse Fftm: three launches)
     from openvsip_b200.vsip import Fftm, fft_fwd, fft_inv, replica_spectrum, vmmul
@@ -477,7 +478,7 @@ def batch_block(args, world: int = 1, rank: int = 0, barrier=lambda: None) -> di
         "rel_l2_vs_fp64": {"max": max_err, "median_rank0": float(np.median(errs)), "jobs_checked": len(errs),
                            "rows_per_job": 3, "tolerance": 2e-6},
         "tuning": tune, "batch": bt.info(), "gpu_launches_per_step": 1,
-        "per_call": {"ms": per_call_ms, "value": all_samples / (per_call_ms / 1e3), "launches_per_step": len(plans),
+        "per_call": {"ms": per_call_ms, "value": all_samples / (per_call_ms / 1e3), "launches_per_step": n_plans,
                      "how": "one fused Fastconv launch per job, plans prepared beforehand, device data"},
         "batch_over_per_call": per_call_ms / mean,
         "per_call_phased": {"ms": phased_ms, "value": all_samples / (phased_ms / 1e3), "launches_per_step": 3 * len(xs),
