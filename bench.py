@@ -567,11 +567,17 @@ def serve_block(args) -> dict:
 
     consumer = threading.Thread(target=consume)
     with Server(replicas, memory_budget=40e9, slots=2) as srv:
-        # warm-up (not timed): every length through both slots once, so module
-        # loading and the allocator's first growth are not in the latencies
+        # warm-up (not timed): every length through both slots once, then a burst of
+        # mixed jobs that fills large launches, and one check of each length, so module
+        # loading and the allocators' first growth are not in the latencies
         warm = [srv.submit(pool[n][:512], by_n[n][0]) for n in sizes for _ in range(2)]
+        warm += [srv.submit(pool[n][:p], by_n[n][0]) for p, n in shapes[:400]]
         for r in warm:
             r.wait(timeout=600)
+        with torch.cuda.stream(check_stream):
+            for n in sizes:
+                torch.linalg.vector_norm(pool[n][:512].to(torch.complex128) - refs[by_n[n][0]][:512])
+        check_stream.synchronize()
         del warm
         # keep the cyclic garbage collector out of the timed stream
         import gc
@@ -594,12 +600,17 @@ def serve_block(args) -> dict:
     errs = (torch.stack(nums).cpu().numpy() / np.array(dens)) if nums else np.array([np.nan])
     lat = np.array(lat) * 1e3
     samples = sum(p * n for p, n in shapes)
+    # where in the stream the slow jobs were (arrival time in 10 s buckets)
+    when = (np.array(t_arrive) - t0) // 10
+    by_10s = {f"{int(k) * 10}-{int(k) * 10 + 10}s": round(float(np.percentile(lat[when == k], 99)), 3)
+              for k in np.unique(when)}
     return {
         "workload": SERVE_WORKLOAD.format(rate=rate, seconds=seconds), "jobs": count, "launches": launches,
         "offered_samples_per_s": samples / seconds, "value": samples / wall, "unit": "complex samples/s",
         "wall_s": wall,
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                       "max": float(lat.max())},
+                       "max": float(lat.max()), "jobs_over_10ms": int((lat > 10).sum()),
+                       "p99_by_arrival": by_10s},
         "rel_l2_vs_fp64": {"max": float(errs.max()), "median": float(np.median(errs)), "jobs_checked": int(errs.size),
                            "check_every": every, "tolerance": 2e-6,
                            "how": "FP64 numpy/scipy result of each job's rows, compared on a side CUDA stream"},
@@ -824,9 +835,17 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_value = samples_step * e2e_steps * world / shard.max_over_ranks(e2e_s)
 
-    # the uneven batch on every rank (jobs partitioned across ranks), the served stream on one GPU
+    # the served stream on one GPU (first: its latencies are the most sensitive to what ran
+    # before), then the uneven batch on every rank (jobs partitioned across ranks)
+    serve = None
+    if world == 1 and not args.no_serve:
+        import gc
+        torch.cuda.synchronize()
+        gc.collect()
+        serve = serve_block(args)
+        gc.collect()
+        torch.cuda.empty_cache()
     batch = None if args.no_batch else batch_block(args, world, rank, barrier)
-    serve = serve_block(args) if (world == 1 and not args.no_serve) else None
 
     if rank == 0:
         cpu = None

@@ -524,7 +524,9 @@ int fcb_batch_set_jobs(fcb_batch b, const fcb_job *jobs, int njobs, int order)
     b->d_jobs = nullptr;
     b->h_jobs = nullptr;
     b->jobs_cap = 0;
-    const size_t cap = std::max<size_t>(hj.size(), 64);
+    // grown geometrically: every growth frees the old table (a device-wide
+    // synchronisation), so a job count that ramps up must not regrow it each call
+    const size_t cap = std::max<size_t>(hj.size(), std::max<size_t>(64, 2 * b->jobs_cap));
     cudaError_t e = cudaMalloc(&b->d_jobs, sizeof(BatchJob) * cap);
     if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "job table");
     e = cudaMallocHost(&b->h_jobs, sizeof(BatchJob) * cap);

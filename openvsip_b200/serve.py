@@ -72,12 +72,22 @@ class Server:
                 torch.empty(int(reserve) // 8, dtype=torch.complex64, device="cuda")
         torch.cuda.synchronize()
         self.batches = []
+        # one spare 256-sample replica per batch, used only to size the job
+        # tables below (its id follows the callers' replicas)
+        import numpy as np
+        spare = np.ones(256, dtype=np.complex64)
+        dummy = torch.zeros(1, 256, dtype=torch.complex64, device="cuda")
         for st in self.streams:
             b = Batch(threads)
             ids = [b.add_replica(r, kind=kind) for r in replicas]
             assert ids == list(range(len(replicas)))
+            sid = b.add_replica(spare, kind="spectrum")
             b.set_stream(st.cuda_stream)
+            # size the job table for max_jobs now: growing it while serving frees the old
+            # table, which synchronises the whole device and stalls the other slot
+            b.set_jobs([(dummy, dummy, sid)] * self.max_jobs, direct=True)
             self.batches.append(b)
+        torch.cuda.synchronize()
         self.nreplicas = len(replicas)
         self._pending = collections.deque()
         self._inflight = [None] * slots  # (requests, event) per slot
