@@ -24,14 +24,15 @@ def test_served_results_equal_alone_results(oracle):
         p = int(rng.integers(1, 40))
         x = torch.view_as_complex(torch.randn(p, n, 2, device="cuda"))
         jobs.append((x, k))
-    # the batch kernels run 32 samples per thread: the alone results use the
-    # same kernels (at 16384 samples the single-job default is the wide one)
-    with pinned_variant(16384, 2, 512):
+    # the server's batch kernel is the wide one (64 samples per thread at 16384
+    # and 32768, 32 below): the alone results use the single-job variants with
+    # the same arithmetic
+    with pinned_variant(16384, 2, -256), pinned_variant(32768, 2, -256):
         alone = [Fastconv(chirps[k], x.shape[0], kind="matched")(x) for x, k in jobs]
     torch.cuda.synchronize()
     # a small budget so that admission has to wait for memory to free up
     budget = 3 * max(2 * x.numel() * 8 for x, _ in jobs)
-    with Server(chirps, memory_budget=budget, slots=2, max_jobs=8) as srv:
+    with Server(chirps, memory_budget=budget, slots=2, max_jobs=8, threads=-256) as srv:
         reqs = [srv.submit(x, k) for x, k in jobs]
         outs = [r.wait(timeout=60) for r in reqs]
         assert srv.launches > 1 and srv.launches < len(jobs)  # batched, in several launches
