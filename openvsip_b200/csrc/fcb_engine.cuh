@@ -58,7 +58,9 @@ constexpr int kMaxLogN = 16;
 
 // ---------------------------------------------------------------------------
 // Schedule of a length-2^LOGN row transform on CTAs of THREADS threads.
-template <int LOGN, int THREADS, int EPTW = 32>
+// ONE_PER_SM = 1: the caller runs one CTA per SM whatever the schedule's own
+// occupancy (a persistent kernel), so the halves of the CTA are staggered.
+template <int LOGN, int THREADS, int EPTW = 32, int ONE_PER_SM = 0>
 struct Sched
 {
   static constexpr int T = THREADS;
@@ -101,7 +103,7 @@ struct Sched
   static constexpr int MINB = (EPTW == 32 ? 512 : 256) / THREADS;
   // With one CTA per SM its two halves run out of phase through the
   // sub-problem stages (see row_tile)
-  static constexpr bool STAGGER = MINB == 1 && NS >= 3;
+  static constexpr bool STAGGER = (MINB == 1 || ONE_PER_SM) && NS >= 3;
 };
 
 
@@ -463,10 +465,10 @@ __device__ __forceinline__ void half_wait()
 // while consecutive tiles have the same length).  The caller guarantees that
 // no thread of the CTA (or of the CS CTAs) still reads the slot array of a
 // previous tile.
-template <int LOGN, int MODE, int THREADS, int EPTW = 32>
+template <int LOGN, int MODE, int THREADS, int EPTW = 32, int ONE_PER_SM = 0>
 __device__ __forceinline__ void row_tile(const RowArgs &a, long long tile, int rank, int rank_base, bool copy_tw)
 {
-  using S = Sched<LOGN, THREADS, EPTW>;
+  using S = Sched<LOGN, THREADS, EPTW, ONE_PER_SM>;
   constexpr int RB = S::RB, LRB = S::LRB;
   constexpr int SIGN = (MODE == kInv) ? +1 : -1;  // direction of the first pass
   constexpr bool CHIRP = MODE == kChirpconv;
