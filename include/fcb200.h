@@ -244,8 +244,7 @@ typedef struct
 /* threads: 256 or 512 (CTAs of 32 samples per thread; clusters of 4 x 256 or
  * 2 x 512 threads share a 32768-sample row), -256 (the wide kernel: one
  * 256-thread CTA per SM; rows of 16384 and 32768 samples run 64 samples per
- * thread, 32768 on clusters of two CTAs), or 0 for the default (the wide
- * kernel). */
+ * thread, 32768 on clusters of two CTAs), or 0 for the default (512). */
 FCB_API int fcb_batch_create(int threads, fcb_batch *batch);
 /* Keep a replica resident on the device (spectrum built in FP64 for the time
  * kinds); returns its id. */

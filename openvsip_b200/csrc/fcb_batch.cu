@@ -119,7 +119,6 @@ __global__ void __launch_bounds__(T, WIDE ? 1 : 512 / T)
   constexpr int W = sizeof(RowArgs) / 8;
   static_assert(sizeof(RowArgs) % 8 == 0 && W <= T, "job arguments are copied as 8-byte words");
   const int hw_rank = HC ? (int)cg::this_cluster().block_rank() : 0;
-  const int warp = threadIdx.x >> 5;
   const bool smem_jobs = njobs <= kSmemJobs;
   if (smem_jobs)
     for (int i = threadIdx.x; i < njobs; i += T) s_begin[i] = jobs[i].unit_begin;
@@ -136,45 +135,62 @@ __global__ void __launch_bounds__(T, WIDE ? 1 : 512 / T)
     }
     return lo;
   };
-  int cur_logn = -1, cur_job = -1;
-  int it = 0;
-  bool cluster_phase = HC && cl_units > 0;
+  // loop state kept in shared memory (CTA-uniform), so that it holds no
+  // registers across the tile code
+  __shared__ int s_state[4];  // cur_logn, cur_job, it, cluster_phase
+  if (threadIdx.x == 0)
+  {
+    s_state[0] = -1;
+    s_state[1] = -1;
+    s_state[2] = 0;
+    s_state[3] = (HC && cl_units > 0) ? 1 : 0;
+  }
+  __syncthreads();
   // Thread 0 (of rank 0 in the cluster phase) asks for the next unit while the
   // current one runs, so the ticket's round trip is off the critical path.
   long long next = 0;
-  if (threadIdx.x == 0 && (cluster_phase ? hw_rank == 0 : true))
-    next = (long long)atomicAdd(&ticket[cluster_phase ? 0 : 1], 1ULL);
+  if (threadIdx.x == 0 && (s_state[3] ? hw_rank == 0 : true))
+    next = (long long)atomicAdd(&ticket[s_state[3] ? 0 : 1], 1ULL);
   // one loop and one call of the tile code (two inlined copies of it would
   // not fit the wide kernel's registers)
 #pragma unroll 1
-  for (;; ++it)
+  for (;;)
   {
+    const int it = s_state[2];
+    const int cur_logn = s_state[0], cur_job = s_state[1];
+    const bool cluster_phase = s_state[3] != 0;
+    const int rank = HC ? (int)cg::this_cluster().block_rank() : 0;
     const int slot = it & 1;
     long long u;
     int lo, logn, tpu, r;
     if (cluster_phase)
     {
-      if (hw_rank == 0 && threadIdx.x == 0) s_unit[slot] = next;
+      if (rank == 0 && threadIdx.x == 0) s_unit[slot] = next;
       cluster_sync();
       u = ld_cluster_s64(cluster_addr(smem_addr(&s_unit[slot]), 0));
       if (u >= cl_units)
       {
         cluster_sync();  // rank 0 stays until every CTA has read
-        cluster_phase = false;
-        if (threadIdx.x == 0) next = (long long)atomicAdd(&ticket[1], 1ULL);
+        if (threadIdx.x == 0)
+        {
+          s_state[3] = 0;
+          s_state[2] = it + 1;
+          next = (long long)atomicAdd(&ticket[1], 1ULL);
+        }
+        __syncthreads();
         continue;
       }
-      if (hw_rank == 0 && threadIdx.x == 0) next = (long long)atomicAdd(&ticket[0], 1ULL);
+      if (rank == 0 && threadIdx.x == 0) next = (long long)atomicAdd(&ticket[0], 1ULL);
       lo = find(u, cur_job >= 0 ? cur_job : 0, ncl - 1);
       logn = jobs[lo].logn;
       tpu = jobs[lo].tiles_per_unit;
-      r = hw_rank;
+      r = rank;
     }
     else
     {
       // warp 0 finds the unit's job before the barrier, while the other warps
       // finish the previous tile
-      if (warp == 0)
+      if ((threadIdx.x >> 5) == 0)
       {
         const long long uu = __shfl_sync(0xffffffffu, next, 0);
         if (uu < solo_units)
@@ -205,10 +221,16 @@ __global__ void __launch_bounds__(T, WIDE ? 1 : 512 / T)
         reinterpret_cast<long long *>(&s_args)[threadIdx.x] =
             reinterpret_cast<const long long *>(&jobs[lo].args)[threadIdx.x];
       __syncthreads();
-      cur_job = lo;
     }
     const bool copy = logn != cur_logn;
-    cur_logn = logn;
+    // every thread has read this iteration's state (the barriers above); the next
+    // iteration reads it after the tile's own barriers
+    if (threadIdx.x == 0)
+    {
+      s_state[0] = logn;
+      s_state[1] = lo;
+      s_state[2] = it + 1;
+    }
     run_unit<T, CSMAX, WIDE>(s_args, logn, u - begin(lo), tpu, r, copy);
   }
 }
@@ -362,9 +384,9 @@ int fcb_batch_create(int threads, fcb_batch *out)
 {
   if (!out) return set_error(FCB_ERR_INVALID, "batch pointer is NULL");
   *out = nullptr;
-  // default: the wide kernel (measured fastest on the uneven 512-job mix: 0.330 of HBM against
-  // 0.326 for 512 threads)
-  if (threads == 0) threads = -256;
+  // default: 512 threads (measured fastest on the uneven 512-job mix: 0.337 of HBM against
+  // 0.3325 for the wide kernel)
+  if (threads == 0) threads = 512;
   if (threads != 256 && threads != 512 && threads != -256)
     return set_error(FCB_ERR_INVALID, "threads must be 0, 256, 512 or -256 (wide)");
   int count = 0;
