@@ -163,7 +163,10 @@ FCB_API int fcb_exec(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf3
  * untouched until fcb_sync returns.  Calls queued back to back on one plan run
  * in order and overlap: the next call's copies in run while the previous
  * call's last copies out drain (a streaming caller keeps the PCIe link busy in
- * both directions across calls).  Host buffers should be pinned.  2-D plans
+ * both directions across calls).  A queued call copies in chunks of twice the
+ * size fcb_exec uses, without fcb_exec's smaller chunks at both ends of the
+ * call (those shorten one call's fill and drain, which a stream of calls
+ * overlaps anyway).  Host buffers should be pinned.  2-D plans
  * run host calls synchronously.  No reference counterpart (the reference's
  * Fftm calls are synchronous).  With where = FCB_DEVICE it is fcb_exec. */
 FCB_API int fcb_exec_async(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out,

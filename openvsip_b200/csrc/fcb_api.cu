@@ -29,11 +29,12 @@ struct fcb_plan_s
   cudaStream_t stream = nullptr;  // current stream (own or caller's)
   // host calls: chunks pipelined through kMaxStage device buffers, copies in
   // on cin, kernels on the plan stream, copies out on cout
-  static constexpr int kMaxStage = 4;
+  static constexpr int kMaxStage = 8;
   cudaStream_t cin = nullptr, cout = nullptr;
   float2 *stage[kMaxStage] = {};
   long long stage_rows = 0;
   int nstage = 0;
+  int stage_next = 0;  // buffer of the next call's first chunk (the rotation continues across calls)
   cudaEvent_t ev_in[kMaxStage] = {}, ev_k[kMaxStage] = {}, ev_out[kMaxStage] = {}, ev_start = nullptr;
   // 2-D FFT (rows x cols): pass 1 transforms rows into a transposed scratch
   // matrix, pass 2 transforms its rows (the columns) back transposed.
@@ -527,7 +528,8 @@ int exec_device(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long
 }
 
 // Host staging shape: chunk bytes and pipeline depth.  FCB200_STAGE_MB and
-// FCB200_STAGES override the defaults (16 MB, 3 buffers).
+// FCB200_STAGES override the defaults (16 MB, 4 buffers; queued calls use
+// chunks of twice the size).
 long long stage_bytes()
 {
   static const long long v = [] {
@@ -541,7 +543,7 @@ int stage_depth()
 {
   static const int v = [] {
     const char *e = std::getenv("FCB200_STAGES");
-    const int d = e ? std::atoi(e) : 3;
+    const int d = e ? std::atoi(e) : 4;
     return std::min(std::max(d, 2), (int)fcb_plan_s::kMaxStage);
   }();
   return v;
@@ -589,27 +591,39 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
               long long rows, bool sync = true)
 {
   const size_t row_bytes = sizeof(float2) * (size_t)p->n;
-  long long chunk = std::max<long long>(1, stage_bytes() / (long long)row_bytes);
-  if (p->k && p->k->cluster == 1) chunk = std::max<long long>(chunk, p->k->rows_per_cta);
+  // A queued call (sync = false) is expected to have neighbours on the link:
+  // it moves twice the chunk size per copy and skips the ramps below (fewer,
+  // larger copies; the fill and drain overlap the neighbouring calls).  The
+  // staging buffers always hold the larger chunk, so that switching between
+  // waiting and queued calls never reallocates them (a cudaFree waits for
+  // the whole device).
+  const long long base = std::max<long long>(1, stage_bytes() / (long long)row_bytes);
+  long long chunk = sync ? base : 2 * base;
+  long long alloc = 2 * base;
+  if (p->k && p->k->cluster == 1)
+  {
+    chunk = std::max<long long>(chunk, p->k->rows_per_cta);
+    alloc = std::max<long long>(alloc, p->k->rows_per_cta);
+  }
   chunk = std::min(chunk, rows);
   const int depth = stage_depth();
-  int rc = ensure_staging(p, chunk, depth);
+  int rc = ensure_staging(p, std::min(alloc, rows), depth);
   if (rc) return rc;
   // nothing starts before earlier work on the plan stream
   cudaEventRecord(p->ev_start, p->stream);
   cudaStreamWaitEvent(p->cin, p->ev_start, 0);
   cudaStreamWaitEvent(p->cout, p->ev_start, 0);
-  // Chunk sizes ramp up over the first chunks and down over the last ones
-  // (1/8, 1/4, 1/2 of a full chunk), so the first copy out and the last copy
-  // in overlap the other direction sooner: the link idles in one direction
-  // only for a small chunk at each end of the call.
+  // Chunk sizes of a call that waits for its result ramp up over the first
+  // chunks and down over the last ones (1/8, 1/4, 1/2 of a full chunk), so the
+  // first copy out and the last copy in overlap the other direction sooner:
+  // the link idles in one direction only for a small chunk at each end.
   const long long unit = std::max<long long>(1, (p->k && p->k->cluster == 1) ? p->k->rows_per_cta : 1);
   std::vector<long long> sizes;
   {
     const long long ramp[3] = {chunk / 8, chunk / 4, chunk / 2};
     long long head = 0;
     for (long long v : ramp) head += std::max(unit, v);
-    if (rows >= 2 * head + chunk)
+    if (sync && rows >= 2 * head + chunk)
     {
       long long left = rows;
       for (long long v : ramp) { sizes.push_back(std::max(unit, v)); left -= sizes.back(); }
@@ -621,9 +635,14 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
       for (long long left = rows; left > 0; left -= sizes.back()) sizes.push_back(std::min(chunk, left));
   }
   long long r0 = 0;
+  // The buffer rotation continues from the previous call, so that a call
+  // queued behind another one (fcb_exec_async) fills first the buffers whose
+  // copies out finished earliest instead of waiting for the last ones.
+  const int b0 = p->stage_next % depth;
+  p->stage_next = (int)((b0 + sizes.size()) % depth);
   for (size_t c = 0; c < sizes.size(); r0 += sizes[c], ++c)
   {
-    const int b = (int)(c % depth);
+    const int b = (int)((b0 + c) % depth);
     const long long nr = sizes[c];
     float2 *buf = p->stage[b];
     // buffer drained: by this call's copy out of chunk c - depth, or by the last

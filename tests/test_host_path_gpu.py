@@ -1,7 +1,8 @@
 """The host-buffer path (numpy in, numpy out) on shapes large enough that rows
-stream through the device in many chunks, with the chunk sizes ramped at both
-ends of the call: results must be identical to the device-pointer path (the
-same kernels per row) and match FP64 on sampled rows (relative L2 <= 2e-6)."""
+stream through the device in many chunks (ramped at both ends of a waiting
+call; twice as large, with no ramp, for queued calls): results must be
+identical to the device-pointer path (the same kernels per row) and match FP64
+on sampled rows (relative L2 <= 2e-6)."""
 import numpy as np
 import pytest
 
@@ -84,3 +85,26 @@ def test_submitted_host_calls_equal_single_calls(oracle, rows, n, steps):
         fc.submit(x, out)
     fc.sync()
     np.testing.assert_array_equal(out, fc(xs[-1]))
+
+
+def test_waiting_and_queued_calls_interleaved():
+    # a waiting call first (staging sized for its chunks), then queued calls
+    # (chunks twice as large: the staging grows), a waiting call between queued
+    # ones, and queued calls again: every output equals the device path's
+    import torch
+    rows, n = 900, 16384
+    rng = np.random.default_rng(77)
+    rep = crandn(rng, (n,))
+    fc = Fastconv(rep, rows)
+    xs = [torch.from_numpy(crandn(rng, (rows, n))).pin_memory().numpy() for _ in range(4)]
+    want = [_device(fc, x) for x in xs]
+    ys = [torch.empty((rows, n), dtype=torch.complex64).pin_memory().numpy() for _ in range(4)]
+    np.testing.assert_array_equal(fc(xs[0]), want[0])
+    fc.submit(xs[1], ys[1])
+    fc.submit(xs[2], ys[2])
+    np.testing.assert_array_equal(fc(xs[3]), want[3])
+    fc.submit(xs[0], ys[0])
+    fc.submit(xs[3], ys[3])
+    fc.sync()
+    for y, w in zip(ys, want):
+        np.testing.assert_array_equal(y, w)
