@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 
-SOURCES = ["fcb200.cu", "fcb_api.cu", "fcb_batch.cu", "fcb_bluestein.cu", "fcb_real.cu"]
+SOURCES = ["fcb200.cu", "fcb_api.cu", "fcb_batch.cu", "fcb_bluestein.cu", "fcb_real.cu", "fcb_hostcopy.cu"]
 
 
 def nvcc() -> str:
@@ -69,7 +69,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         list(ex.map(run, jobs))
     if force or jobs or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

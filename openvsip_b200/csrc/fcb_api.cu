@@ -35,6 +35,12 @@ struct fcb_plan_s
   long long stage_rows = 0;
   int nstage = 0;
   int stage_next = 0;  // buffer of the next call's first chunk (the rotation continues across calls)
+  // host calls on pageable memory: pinned host buffers per staging buffer
+  // (hstage[0] in, hstage[1] out), filled and drained by the copy threads
+  float2 *hstage[2][kMaxStage] = {};
+  size_t hstage_bytes[2] = {0, 0};
+  int nhstage[2] = {0, 0};
+  cudaEvent_t ev_h[2][kMaxStage] = {};  // a pinned buffer's last copy (in: to the device; out: from it)
   cudaEvent_t ev_in[kMaxStage] = {}, ev_k[kMaxStage] = {}, ev_out[kMaxStage] = {}, ev_start = nullptr;
   // 2-D FFT (rows x cols): pass 1 transforms rows into a transposed scratch
   // matrix, pass 2 transforms its rows (the columns) back transposed.
@@ -143,6 +149,11 @@ void plan_free(fcb_plan p)
   plan_free(p->sub2d[1]);
   cudaFree(p->rep);
   for (auto b : p->stage) cudaFree(b);
+  for (auto &dir : p->hstage)
+    for (auto b : dir) cudaFreeHost(b);
+  for (auto &dir : p->ev_h)
+    for (auto ev : dir)
+      if (ev) cudaEventDestroy(ev);
   for (int d = 0; d < 2; ++d)
   {
     plan_free(p->inner[d]);
@@ -395,6 +406,111 @@ int exec_real_device(fcb_plan p, const void *in, long long in_rs, void *out, lon
 // A host-buffer call returns only once none of its copies is queued or running,
 // on an error too: its caller may free or reuse the host buffers as soon as
 // the call returns.  Waits for the plan's streams and keeps the first error.
+long long stage_bytes();
+int stage_depth();
+
+// Pinned host buffers for pageable copies in direction d (0: to the device,
+// 1: from it): `depth` buffers of at least `bytes` each, and their events.
+int ensure_host_staging(fcb_plan p, int d, size_t bytes, int depth)
+{
+  if (!p->ev_h[d][0])
+    for (int i = 0; i < fcb_plan_s::kMaxStage; ++i)
+    {
+      const cudaError_t e = cudaEventCreateWithFlags(&p->ev_h[d][i], cudaEventDisableTiming);
+      if (e != cudaSuccess) return cuda_error(e, "staging events");
+    }
+  if (p->hstage_bytes[d] >= bytes && p->nhstage[d] >= depth) return FCB_OK;
+  for (auto &b : p->hstage[d])
+  {
+    cudaFreeHost(b);
+    b = nullptr;
+  }
+  p->hstage_bytes[d] = 0;
+  p->nhstage[d] = 0;
+  for (int i = 0; i < depth; ++i)
+  {
+    const cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&p->hstage[d][i]), bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "pinned staging buffer: %s", cudaGetErrorString(e));
+  }
+  p->hstage_bytes[d] = bytes;
+  p->nhstage[d] = depth;
+  return FCB_OK;
+}
+
+// Host -> device copy of `rows` rows of `rb` bytes (pitches in bytes) on
+// stream st.  Pinned host memory moves directly.  Pageable host memory moves
+// through the plan's pinned buffers in chunks of about the staging size, each
+// copied by the copy threads while the copy engine moves the previous one;
+// returns once the last chunk is queued.
+int copy_h2d(fcb_plan p, void *dev, size_t dp, const void *host, size_t hp, size_t rb, size_t rows,
+             cudaStream_t st)
+{
+  cudaError_t e;
+  if (!host_pageable(host, hp * (rows - 1) + rb))
+  {
+    e = cudaMemcpy2DAsync(dev, dp, host, hp, rb, rows, cudaMemcpyHostToDevice, st);
+    return e == cudaSuccess ? FCB_OK : cuda_error(e, "host->device copy");
+  }
+  const int depth = stage_depth();
+  const size_t chunk = std::max<size_t>(1, (size_t)stage_bytes() / rb);
+  int rc = ensure_host_staging(p, 0, std::min(chunk, rows) * rb, depth);
+  if (rc) return rc;
+  for (size_t r0 = 0, c = 0; r0 < rows; r0 += chunk, ++c)
+  {
+    const int b = (int)(c % depth);
+    const size_t nr = std::min(chunk, rows - r0);
+    if ((e = cudaEventSynchronize(p->ev_h[0][b])) != cudaSuccess) return cuda_error(e, "host->device copy");
+    host_copy_rows(p->hstage[0][b], rb, static_cast<const char *>(host) + r0 * hp, hp, rb, nr);
+    e = cudaMemcpy2DAsync(static_cast<char *>(dev) + r0 * dp, dp, p->hstage[0][b], rb, rb, nr,
+                          cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+    cudaEventRecord(p->ev_h[0][b], st);
+  }
+  return FCB_OK;
+}
+
+// Device -> host copy of `rows` rows of `rb` bytes on stream st, after the work
+// queued on it.  Pageable host memory: through the plan's pinned buffers, the
+// copy threads draining each chunk while the copy engine moves the next ones;
+// returns once the host rows are written.  Pinned host memory: queued only.
+int copy_d2h(fcb_plan p, void *host, size_t hp, const void *dev, size_t dp, size_t rb, size_t rows,
+             cudaStream_t st)
+{
+  cudaError_t e;
+  if (!host_pageable(host, hp * (rows - 1) + rb))
+  {
+    e = cudaMemcpy2DAsync(host, hp, dev, dp, rb, rows, cudaMemcpyDeviceToHost, st);
+    return e == cudaSuccess ? FCB_OK : cuda_error(e, "device->host copy");
+  }
+  const int depth = stage_depth(), lag = depth - 1;
+  const size_t chunk = std::max<size_t>(1, (size_t)stage_bytes() / rb);
+  int rc = ensure_host_staging(p, 1, std::min(chunk, rows) * rb, depth);
+  if (rc) return rc;
+  const size_t nc = (rows + chunk - 1) / chunk;
+  auto drain = [&](size_t c) -> int {
+    const int b = (int)(c % depth);
+    const size_t r0 = c * chunk, nr = std::min(chunk, rows - r0);
+    const cudaError_t e2 = cudaEventSynchronize(p->ev_h[1][b]);
+    if (e2 != cudaSuccess) return cuda_error(e2, "device->host copy");
+    host_copy_rows(static_cast<char *>(host) + r0 * hp, hp, p->hstage[1][b], rb, rb, nr);
+    return FCB_OK;
+  };
+  for (size_t c = 0; c < nc; ++c)
+  {
+    const int b = (int)(c % depth);
+    const size_t r0 = c * chunk, nr = std::min(chunk, rows - r0);
+    // the pinned buffer's previous chunk was drained lag chunks ago
+    e = cudaMemcpy2DAsync(p->hstage[1][b], rb, static_cast<const char *>(dev) + r0 * dp, dp, rb, nr,
+                          cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    cudaEventRecord(p->ev_h[1][b], st);
+    if (c >= (size_t)lag && (rc = drain(c - lag))) return rc;
+  }
+  for (size_t c = nc > (size_t)lag ? nc - lag : 0; c < nc; ++c)
+    if ((rc = drain(c))) return rc;
+  return FCB_OK;
+}
+
 int host_done(fcb_plan p, int rc, const char *what)
 {
   const cudaStream_t ss[3] = {p->cin, p->cout, p->stream};
@@ -434,16 +550,14 @@ int exec_real_host(fcb_plan p, const void *in, long long in_rs, void *out, long 
   for (long long r0 = 0; r0 < rows; r0 += chunk)
   {
     const long long nr = std::min(chunk, rows - r0);
-    cudaError_t e = cudaMemcpy2DAsync(p->rstage[0], in_el * (size_t)in_pitch, src + in_el * (size_t)(r0 * in_rs),
-                                      in_el * (size_t)in_rs, in_el * (size_t)in_cols, (size_t)nr,
-                                      cudaMemcpyHostToDevice, p->stream);
-    if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "real FFT (host)");
-    int rc = exec_real_device(p, p->rstage[0], in_pitch, p->rstage[1], out_pitch, nr, p->stream);
+    int rc = copy_h2d(p, p->rstage[0], in_el * (size_t)in_pitch, src + in_el * (size_t)(r0 * in_rs),
+                      in_el * (size_t)in_rs, in_el * (size_t)in_cols, (size_t)nr, p->stream);
     if (rc) return host_done(p, rc, "real FFT (host)");
-    e = cudaMemcpy2DAsync(dst + out_el * (size_t)(r0 * out_rs), out_el * (size_t)out_rs, p->rstage[1],
-                          out_el * (size_t)out_pitch, out_el * (size_t)out_cols, (size_t)nr,
-                          cudaMemcpyDeviceToHost, p->stream);
-    if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "real FFT (host)");
+    rc = exec_real_device(p, p->rstage[0], in_pitch, p->rstage[1], out_pitch, nr, p->stream);
+    if (rc) return host_done(p, rc, "real FFT (host)");
+    rc = copy_d2h(p, dst + out_el * (size_t)(r0 * out_rs), out_el * (size_t)out_rs, p->rstage[1],
+                  out_el * (size_t)out_pitch, out_el * (size_t)out_cols, (size_t)nr, p->stream);
+    if (rc) return host_done(p, rc, "real FFT (host)");
   }
   return host_done(p, FCB_OK, "real FFT (host)");
 }
@@ -587,10 +701,20 @@ int ensure_staging(fcb_plan p, long long chunk_rows, int depth)
 // by events, so both copy directions and the kernels overlap and the PCIe link
 // stays busy in both directions; a buffer is refilled once its copy out is done.
 // sync = false (fcb_exec_async): return once everything is queued.
+int exec_host_staged(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
+                     long long rows, bool stage_in, bool stage_out);
+
 int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
               long long rows, bool sync = true)
 {
   const size_t row_bytes = sizeof(float2) * (size_t)p->n;
+  {
+    // pageable host memory goes through the plan's pinned buffers
+    const size_t in_span = sizeof(float2) * (size_t)((rows - 1) * in_rs + p->n);
+    const size_t out_span = sizeof(float2) * (size_t)((rows - 1) * out_rs + p->n);
+    const bool stage_in = host_pageable(in, in_span), stage_out = host_pageable(out, out_span);
+    if (stage_in || stage_out) return exec_host_staged(p, in, in_rs, out, out_rs, rows, stage_in, stage_out);
+  }
   // A queued call (sync = false) is expected to have neighbours on the link:
   // it moves twice the chunk size per copy and skips the ramps below (fewer,
   // larger copies; the fill and drain overlap the neighbouring calls).  The
@@ -673,6 +797,99 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? FCB_OK : cuda_error(e, "fcb_exec_async (host)");
   }
+  return host_done(p, FCB_OK, "fcb_exec (host)");
+}
+
+// Host call with pageable input and/or output: each chunk is copied by the
+// copy threads into a pinned buffer of the plan, moved in, transformed, moved
+// out into another pinned buffer and copied to the caller's rows, while the
+// copy engines and the kernels work on the neighbouring chunks.  A pinned side
+// moves directly.  Returns when the output is written, queued or not.
+int exec_host_staged(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
+                     long long rows, bool stage_in, bool stage_out)
+{
+  const size_t row_bytes = sizeof(float2) * (size_t)p->n;
+  long long chunk = std::max<long long>(1, stage_bytes() / (long long)row_bytes);
+  long long alloc = 2 * chunk;  // the device buffers as the pinned path sizes them
+  if (p->k && p->k->cluster == 1)
+  {
+    chunk = std::max<long long>(chunk, p->k->rows_per_cta);
+    alloc = std::max<long long>(alloc, p->k->rows_per_cta);
+  }
+  chunk = std::min(chunk, rows);
+  const int depth = stage_depth();
+  int rc = ensure_staging(p, std::min(alloc, rows), depth);
+  if (rc) return rc;
+  if (stage_in && (rc = ensure_host_staging(p, 0, row_bytes * (size_t)chunk, depth))) return rc;
+  if (stage_out && (rc = ensure_host_staging(p, 1, row_bytes * (size_t)chunk, depth))) return rc;
+  cudaEventRecord(p->ev_start, p->stream);
+  cudaStreamWaitEvent(p->cin, p->ev_start, 0);
+  cudaStreamWaitEvent(p->cout, p->ev_start, 0);
+  const long long nc = (rows + chunk - 1) / chunk;
+  const int b0 = p->stage_next % depth;
+  p->stage_next = (int)((b0 + nc) % depth);
+  const int lag = depth - 1;  // chunks between a chunk's copy in and its copy out on the host
+  auto buf_of = [&](long long c) { return (int)((b0 + c) % depth); };
+  // copy chunk d's result from its pinned buffer to the caller's rows
+  auto drain = [&](long long d) -> int {
+    const int b = buf_of(d);
+    const long long r0 = d * chunk, nr = std::min(chunk, rows - r0);
+    const cudaError_t e = cudaEventSynchronize(p->ev_h[1][b]);
+    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+    host_copy_rows(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, p->hstage[1][b], row_bytes, row_bytes,
+                   (size_t)nr);
+    return FCB_OK;
+  };
+  for (long long c = 0; c < nc; ++c)
+  {
+    const int b = buf_of(c);
+    const long long r0 = c * chunk, nr = std::min(chunk, rows - r0);
+    const float2 *src = in + r0 * in_rs;
+    long long src_rs = in_rs;
+    if (stage_in)
+    {
+      // the pinned buffer's previous chunk has moved in
+      cudaError_t e = cudaEventSynchronize(p->ev_h[0][b]);
+      if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "fcb_exec (host)");
+      host_copy_rows(p->hstage[0][b], row_bytes, src, sizeof(float2) * (size_t)in_rs, row_bytes, (size_t)nr);
+      src = p->hstage[0][b];
+      src_rs = p->n;
+    }
+    float2 *buf = p->stage[b];
+    cudaStreamWaitEvent(p->cin, p->ev_out[b], 0);
+    cudaError_t e = src_rs == p->n
+                      ? cudaMemcpyAsync(buf, src, row_bytes * (size_t)nr, cudaMemcpyHostToDevice, p->cin)
+                      : cudaMemcpy2DAsync(buf, row_bytes, src, sizeof(float2) * (size_t)src_rs, row_bytes, (size_t)nr,
+                                          cudaMemcpyHostToDevice, p->cin);
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "fcb_exec (host)");
+    cudaEventRecord(p->ev_in[b], p->cin);
+    if (stage_in) cudaEventRecord(p->ev_h[0][b], p->cin);
+    cudaStreamWaitEvent(p->stream, p->ev_in[b], 0);
+    rc = exec_device(p, buf, p->n, buf, p->n, nr, r0, p->stream, 0);
+    if (rc) return host_done(p, rc, "fcb_exec (host)");
+    cudaEventRecord(p->ev_k[b], p->stream);
+    cudaStreamWaitEvent(p->cout, p->ev_k[b], 0);
+    // the output's pinned buffer was drained on the host depth chunks ago
+    e = stage_out ? cudaMemcpyAsync(p->hstage[1][b], buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
+        : out_rs == p->n
+          ? cudaMemcpyAsync(out + r0 * out_rs, buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
+          : cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,
+                              (size_t)nr, cudaMemcpyDeviceToHost, p->cout);
+    if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "fcb_exec (host)");
+    cudaEventRecord(p->ev_out[b], p->cout);
+    if (stage_out) cudaEventRecord(p->ev_h[1][b], p->cout);
+    if (stage_out && c >= lag)
+    {
+      rc = drain(c - lag);
+      if (rc) return host_done(p, rc, "fcb_exec (host)");
+    }
+  }
+  if (stage_out)
+    for (long long d = std::max<long long>(0, nc - lag); d < nc; ++d)
+    {
+      rc = drain(d);
+      if (rc) return host_done(p, rc, "fcb_exec (host)");
+    }
   return host_done(p, FCB_OK, "fcb_exec (host)");
 }
 
@@ -865,15 +1082,12 @@ int exec_impl(fcb_plan p, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out, lo
     if (!p->stage2d_in && (e = cudaMalloc(&p->stage2d_in, bytes)) != cudaSuccess)
       return set_error(FCB_ERR_NOMEM, "staging buffer: %s", cudaGetErrorString(e));
     const size_t rb = sizeof(float2) * (size_t)p->cols2d;
-    e = cudaMemcpy2DAsync(p->stage2d_in, rb, i2, sizeof(float2) * (size_t)in_rs, rb, (size_t)p->rows2d,
-                          cudaMemcpyHostToDevice, p->stream);
-    if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "fcb_exec (2-D, host)");
-    int rc = exec_2d(p, p->stage2d_in, p->cols2d, p->stage2d_in, p->cols2d, p->stream);
+    int rc = copy_h2d(p, p->stage2d_in, rb, i2, sizeof(float2) * (size_t)in_rs, rb, (size_t)p->rows2d, p->stream);
     if (rc) return host_done(p, rc, "fcb_exec (2-D, host)");
-    e = cudaMemcpy2DAsync(o2, sizeof(float2) * (size_t)out_rs, p->stage2d_in, rb, rb, (size_t)p->rows2d,
-                          cudaMemcpyDeviceToHost, p->stream);
-    if (e != cudaSuccess) return host_done(p, cuda_error(e, "device->host copy"), "fcb_exec (2-D, host)");
-    return host_done(p, FCB_OK, "fcb_exec (2-D, host)");
+    rc = exec_2d(p, p->stage2d_in, p->cols2d, p->stage2d_in, p->cols2d, p->stream);
+    if (rc) return host_done(p, rc, "fcb_exec (2-D, host)");
+    rc = copy_d2h(p, o2, sizeof(float2) * (size_t)out_rs, p->stage2d_in, rb, rb, (size_t)p->rows2d, p->stream);
+    return host_done(p, rc, "fcb_exec (2-D, host)");
   }
   if (where == FCB_DEVICE) return exec_device(p, i2, in_rs, o2, out_rs, rows, 0, p->stream);
   return exec_host(p, i2, in_rs, o2, out_rs, rows, sync);

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
+
 namespace fcb {
 
 struct RowArgs;
@@ -73,6 +75,12 @@ int c2r_pre(const float2 *x, long long x_rs, float2 *z, long long z_rs, long lon
 int real_expand(const float *x, long long x_rs, float2 *z, long long n, long long rows, cudaStream_t st);
 int herm_expand(const float2 *x, long long x_rs, float2 *z, long long n, long long rows, cudaStream_t st);
 int take_real(const float2 *z, long long n, float *out, long long out_rs, long long rows, cudaStream_t st);
+
+// Host-side copies (fcb_hostcopy.cu): rows x row_bytes between host buffers
+// with the given pitches, split over the copy threads; and whether a host
+// range is pageable (not pinned or registered with CUDA).
+void host_copy_rows(void *dst, size_t dst_pitch, const void *src, size_t src_pitch, size_t row_bytes, size_t rows);
+bool host_pageable(const void *ptr, size_t bytes);
 
 int set_error(int code, const char *fmt, ...);
 const char *error_text();

@@ -108,3 +108,70 @@ def test_waiting_and_queued_calls_interleaved():
     fc.sync()
     for y, w in zip(ys, want):
         np.testing.assert_array_equal(y, w)
+
+
+@pytest.mark.parametrize("pin_in,pin_out", [(False, False), (True, False), (False, True)])
+def test_pageable_host_buffers_staged(oracle, pin_in, pin_out):
+    # pageable sides go through the plan's pinned buffers and the copy threads
+    # (ragged last chunk, strided rows on the pageable side), waiting and
+    # queued calls alike
+    import torch
+    rows, n = 1100, 8192
+    rng = np.random.default_rng(int(pin_in) * 2 + int(pin_out))
+    rep = crandn(rng, (n,))
+    fc = Fastconv(rep, rows)
+    x = crandn(rng, (rows, n))
+    want = _device(fc, x)
+
+    def buf(pinned, like):
+        if pinned:
+            b = torch.empty(like.shape, dtype=torch.complex64).pin_memory().numpy()
+            b[...] = like
+            return b
+        wide = np.zeros((like.shape[0], like.shape[1] + 8), dtype=np.complex64)
+        wide[:, 4:4 + like.shape[1]] = like
+        return wide[:, 4:4 + like.shape[1]]  # row stride n + 8
+
+    xin = buf(pin_in, x)
+    out = buf(pin_out, np.zeros_like(x))
+    fc(xin, out)
+    np.testing.assert_array_equal(out, want)
+    out[...] = 0
+    fc.submit(xin, out)
+    fc.sync()
+    np.testing.assert_array_equal(out, want)
+    if not pin_out:
+        assert not out.base[:, :4].any() and not out.base[:, -4:].any()
+    r = rows - 1
+    assert oracle.rel_l2(out[r:r + 1], oracle.fastconv(x[r:r + 1], rep)) <= RTOL
+
+
+def test_pageable_calls_from_several_threads():
+    # host threads with plans of their own share the copy threads: every
+    # result equals the device path's
+    import threading
+    rng = np.random.default_rng(5)
+    shapes = [(700, 16384), (3000, 2048), (900, 4096)]
+    plans, xs, wants, outs, errs = [], [], [], [None] * 3, []
+    for rows, n in shapes:
+        fc = Fastconv(crandn(rng, (n,)), rows)
+        x = crandn(rng, (rows, n))
+        plans.append(fc)
+        xs.append(x)
+        wants.append(_device(fc, x))
+
+    def work(i):
+        try:
+            for _ in range(3):
+                outs[i] = plans[i](xs[i])
+        except Exception as e:  # pragma: no cover - reported below
+            errs.append(e)
+
+    ts = [threading.Thread(target=work, args=(i,)) for i in range(3)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert not errs
+    for o, w in zip(outs, wants):
+        np.testing.assert_array_equal(o, w)
