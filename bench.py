@@ -834,6 +834,17 @@ def main():
     fc.sync()
     e2e_s = time.perf_counter() - t0
     e2e_value = samples_step * e2e_steps * world / shard.max_over_ranks(e2e_s)
+    # the same calls on pageable numpy arrays (how plain numpy callers and the plugin's
+    # vsip::Matrix blocks arrive): staged through the plan's pinned buffers by host threads
+    pout = np.empty_like(x_host)
+    fc(x_host, pout)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        fc(x_host, pout)
+    e2e_pg_s = time.perf_counter() - t0
+    e2e_pg_value = samples_step * e2e_steps * world / shard.max_over_ranks(e2e_pg_s)
+    del pout
 
     # the served stream on one GPU (first: its latencies are the most sensitive to what ran
     # before), then the uneven batch on every rank (jobs partitioned across ranks)
@@ -890,7 +901,11 @@ def main():
                            "overlapping on the PCIe link",
                     "one_call_at_a_time": {"value": e2e_sync_value, "unit": "complex samples/s",
                                            "how": "Fastconv(host pinned in, host pinned out), each call waits "
-                                                  "for its result"}},
+                                                  "for its result"},
+                    "pageable": {"value": e2e_pg_value, "unit": "complex samples/s",
+                                 "how": "Fastconv(numpy pageable in, numpy pageable out), each call waits for its "
+                                        "result; chunks staged through the plan's pinned buffers by host "
+                                        "threads"}},
             "phased": phased,
             "matrix_of_coefficients": matrix,
             "batch": batch,

@@ -60,6 +60,7 @@ def test_gpu_arm_line():
     assert roof["bound"] == "hbm" and roof["unit"] == "GB/s" and 0 < roof["frac"] == roof["achieved"] / roof["peak"]
     e2e = line["e2e"]
     assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] == e2e["d2h_bytes_per_step"] == 64 * 16384 * 8
+    assert e2e["one_call_at_a_time"]["value"] > 0 and e2e["pageable"]["value"] > 0
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(line["clocks"])
     assert line["rel_l2_vs_fp64"] <= 2e-6
     ph = line["phased"]
