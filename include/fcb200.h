@@ -155,10 +155,12 @@ FCB_API int fcb_plan_fastconv(long long n, long long rows_max, const fcb_cf32 *r
  * call is asynchronous on the plan's stream.  where = FCB_HOST: host pointers;
  * the call copies through the device and returns when out is written.  Pinned
  * (page-locked) host buffers move directly; a pageable buffer is copied chunk
- * by chunk through pinned buffers of the plan by a pool of host threads
- * (FCB200_COPY_THREADS, default three quarters of the host's threads, at most
- * 16), which measured 3-4x faster than handing pageable memory to the CUDA
- * runtime. */
+ * by chunk through pinned buffers shared by all plans of the process (at most
+ * 2 x FCB200_STAGES x FCB200_STAGE_MB, 128 MB by default; one such call at a
+ * time) by a pool of host threads (FCB200_COPY_THREADS, default three quarters
+ * of the host's threads, at most 16), which measured 3-4x faster than handing
+ * pageable memory to the CUDA runtime; if no pinned memory can be had, the
+ * runtime copies it. */
 FCB_API int fcb_exec(fcb_plan plan, const fcb_cf32 *in, long long in_rs, fcb_cf32 *out,
              long long out_rs, long long rows, int where);
 

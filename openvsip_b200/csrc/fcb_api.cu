@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -35,12 +36,9 @@ struct fcb_plan_s
   long long stage_rows = 0;
   int nstage = 0;
   int stage_next = 0;  // buffer of the next call's first chunk (the rotation continues across calls)
-  // host calls on pageable memory: pinned host buffers per staging buffer
-  // (hstage[0] in, hstage[1] out), filled and drained by the copy threads
-  float2 *hstage[2][kMaxStage] = {};
-  size_t hstage_bytes[2] = {0, 0};
-  int nhstage[2] = {0, 0};
-  cudaEvent_t ev_h[2][kMaxStage] = {};  // a pinned buffer's last copy (in: to the device; out: from it)
+  // host calls on pageable memory: each shared pinned staging buffer's last
+  // copy for this plan ([0] to the device, [1] from it)
+  cudaEvent_t ev_h[2][kMaxStage] = {};
   cudaEvent_t ev_in[kMaxStage] = {}, ev_k[kMaxStage] = {}, ev_out[kMaxStage] = {}, ev_start = nullptr;
   // 2-D FFT (rows x cols): pass 1 transforms rows into a transposed scratch
   // matrix, pass 2 transforms its rows (the columns) back transposed.
@@ -149,8 +147,6 @@ void plan_free(fcb_plan p)
   plan_free(p->sub2d[1]);
   cudaFree(p->rep);
   for (auto b : p->stage) cudaFree(b);
-  for (auto &dir : p->hstage)
-    for (auto b : dir) cudaFreeHost(b);
   for (auto &dir : p->ev_h)
     for (auto ev : dir)
       if (ev) cudaEventDestroy(ev);
@@ -403,14 +399,31 @@ int exec_real_device(fcb_plan p, const void *in, long long in_rs, void *out, lon
   return rc;
 }
 
-// A host-buffer call returns only once none of its copies is queued or running,
-// on an error too: its caller may free or reuse the host buffers as soon as
-// the call returns.  Waits for the plan's streams and keeps the first error.
 long long stage_bytes();
 int stage_depth();
 
-// Pinned host buffers for pageable copies in direction d (0: to the device,
-// 1: from it): `depth` buffers of at least `bytes` each, and their events.
+// Pinned host buffers for the staged copies of pageable memory, shared by all
+// plans (one set per process rather than per plan: a program may hold many
+// plans), portable so that plans on any device can use them.  A call that
+// stages holds `mu` from its first copy until none of its copies through
+// these buffers is queued or running.
+constexpr int kNoPinned = -1;  // pinned memory could not be had: copy directly instead
+struct PinnedStaging
+{
+  std::mutex mu;
+  float2 *buf[2][fcb_plan_s::kMaxStage] = {};  // [0] to the device, [1] from it
+  size_t bytes[2] = {0, 0};
+  int count[2] = {0, 0};
+};
+PinnedStaging &pinned()
+{
+  static PinnedStaging *s = new PinnedStaging;  // kept for the process's lifetime
+  return *s;
+}
+
+// With pinned().mu held: `depth` pinned buffers of at least `bytes` bytes for
+// direction d (0: to the device, 1: from it), and the plan's events that track
+// each buffer's last copy.  kNoPinned if the pinned memory could not be had.
 int ensure_host_staging(fcb_plan p, int d, size_t bytes, int depth)
 {
   if (!p->ev_h[d][0])
@@ -419,98 +432,120 @@ int ensure_host_staging(fcb_plan p, int d, size_t bytes, int depth)
       const cudaError_t e = cudaEventCreateWithFlags(&p->ev_h[d][i], cudaEventDisableTiming);
       if (e != cudaSuccess) return cuda_error(e, "staging events");
     }
-  if (p->hstage_bytes[d] >= bytes && p->nhstage[d] >= depth) return FCB_OK;
-  for (auto &b : p->hstage[d])
+  PinnedStaging &ps = pinned();
+  if (ps.bytes[d] >= bytes && ps.count[d] >= depth) return FCB_OK;
+  for (auto &b : ps.buf[d])
   {
     cudaFreeHost(b);
     b = nullptr;
   }
-  p->hstage_bytes[d] = 0;
-  p->nhstage[d] = 0;
+  ps.bytes[d] = 0;
+  ps.count[d] = 0;
   for (int i = 0; i < depth; ++i)
-  {
-    const cudaError_t e = cudaHostAlloc(reinterpret_cast<void **>(&p->hstage[d][i]), bytes, cudaHostAllocDefault);
-    if (e != cudaSuccess) return set_error(FCB_ERR_NOMEM, "pinned staging buffer: %s", cudaGetErrorString(e));
-  }
-  p->hstage_bytes[d] = bytes;
-  p->nhstage[d] = depth;
+    if (cudaHostAlloc(reinterpret_cast<void **>(&ps.buf[d][i]), bytes, cudaHostAllocPortable) != cudaSuccess)
+    {
+      cudaGetLastError();
+      for (auto &b : ps.buf[d])
+      {
+        cudaFreeHost(b);
+        b = nullptr;
+      }
+      return kNoPinned;
+    }
+  ps.bytes[d] = bytes;
+  ps.count[d] = depth;
   return FCB_OK;
 }
 
 // Host -> device copy of `rows` rows of `rb` bytes (pitches in bytes) on
-// stream st.  Pinned host memory moves directly.  Pageable host memory moves
-// through the plan's pinned buffers in chunks of about the staging size, each
-// copied by the copy threads while the copy engine moves the previous one;
-// returns once the last chunk is queued.
+// stream st.  Pinned host memory moves directly (queued only).  Pageable host
+// memory moves through the shared pinned buffers in chunks of about the
+// staging size, each copied by the copy threads while the copy engine moves
+// the previous one; returns once every chunk has arrived.
 int copy_h2d(fcb_plan p, void *dev, size_t dp, const void *host, size_t hp, size_t rb, size_t rows,
              cudaStream_t st)
 {
   cudaError_t e;
-  if (!host_pageable(host, hp * (rows - 1) + rb))
+  if (host_pageable(host, hp * (rows - 1) + rb))
   {
-    e = cudaMemcpy2DAsync(dev, dp, host, hp, rb, rows, cudaMemcpyHostToDevice, st);
-    return e == cudaSuccess ? FCB_OK : cuda_error(e, "host->device copy");
+    std::lock_guard<std::mutex> lk(pinned().mu);
+    const int depth = stage_depth();
+    const size_t chunk = std::max<size_t>(1, (size_t)stage_bytes() / rb);
+    int rc = ensure_host_staging(p, 0, std::min(chunk, rows) * rb, depth);
+    if (rc != kNoPinned)
+    {
+      if (rc) return rc;
+      size_t c = 0;
+      for (size_t r0 = 0; r0 < rows; r0 += chunk, ++c)
+      {
+        const int b = (int)(c % depth);
+        const size_t nr = std::min(chunk, rows - r0);
+        if ((e = cudaEventSynchronize(p->ev_h[0][b])) != cudaSuccess) return cuda_error(e, "host->device copy");
+        host_copy_rows(pinned().buf[0][b], rb, static_cast<const char *>(host) + r0 * hp, hp, rb, nr);
+        e = cudaMemcpy2DAsync(static_cast<char *>(dev) + r0 * dp, dp, pinned().buf[0][b], rb, rb, nr,
+                              cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return cuda_error(e, "host->device copy");
+        cudaEventRecord(p->ev_h[0][b], st);
+      }
+      // the buffers go back to the other plans only once their copies are done
+      for (int b = 0; b < depth; ++b)
+        if ((e = cudaEventSynchronize(p->ev_h[0][b])) != cudaSuccess) return cuda_error(e, "host->device copy");
+      return FCB_OK;
+    }
   }
-  const int depth = stage_depth();
-  const size_t chunk = std::max<size_t>(1, (size_t)stage_bytes() / rb);
-  int rc = ensure_host_staging(p, 0, std::min(chunk, rows) * rb, depth);
-  if (rc) return rc;
-  for (size_t r0 = 0, c = 0; r0 < rows; r0 += chunk, ++c)
-  {
-    const int b = (int)(c % depth);
-    const size_t nr = std::min(chunk, rows - r0);
-    if ((e = cudaEventSynchronize(p->ev_h[0][b])) != cudaSuccess) return cuda_error(e, "host->device copy");
-    host_copy_rows(p->hstage[0][b], rb, static_cast<const char *>(host) + r0 * hp, hp, rb, nr);
-    e = cudaMemcpy2DAsync(static_cast<char *>(dev) + r0 * dp, dp, p->hstage[0][b], rb, rb, nr,
-                          cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) return cuda_error(e, "host->device copy");
-    cudaEventRecord(p->ev_h[0][b], st);
-  }
-  return FCB_OK;
+  e = cudaMemcpy2DAsync(dev, dp, host, hp, rb, rows, cudaMemcpyHostToDevice, st);
+  return e == cudaSuccess ? FCB_OK : cuda_error(e, "host->device copy");
 }
 
 // Device -> host copy of `rows` rows of `rb` bytes on stream st, after the work
-// queued on it.  Pageable host memory: through the plan's pinned buffers, the
+// queued on it.  Pageable host memory: through the shared pinned buffers, the
 // copy threads draining each chunk while the copy engine moves the next ones;
 // returns once the host rows are written.  Pinned host memory: queued only.
 int copy_d2h(fcb_plan p, void *host, size_t hp, const void *dev, size_t dp, size_t rb, size_t rows,
              cudaStream_t st)
 {
   cudaError_t e;
-  if (!host_pageable(host, hp * (rows - 1) + rb))
+  if (host_pageable(host, hp * (rows - 1) + rb))
   {
-    e = cudaMemcpy2DAsync(host, hp, dev, dp, rb, rows, cudaMemcpyDeviceToHost, st);
-    return e == cudaSuccess ? FCB_OK : cuda_error(e, "device->host copy");
+    std::lock_guard<std::mutex> lk(pinned().mu);
+    const int depth = stage_depth(), lag = depth - 1;
+    const size_t chunk = std::max<size_t>(1, (size_t)stage_bytes() / rb);
+    int rc = ensure_host_staging(p, 1, std::min(chunk, rows) * rb, depth);
+    if (rc != kNoPinned)
+    {
+      if (rc) return rc;
+      const size_t nc = (rows + chunk - 1) / chunk;
+      auto drain = [&](size_t c) -> int {
+        const int b = (int)(c % depth);
+        const size_t r0 = c * chunk, nr = std::min(chunk, rows - r0);
+        const cudaError_t e2 = cudaEventSynchronize(p->ev_h[1][b]);
+        if (e2 != cudaSuccess) return cuda_error(e2, "device->host copy");
+        host_copy_rows(static_cast<char *>(host) + r0 * hp, hp, pinned().buf[1][b], rb, rb, nr);
+        return FCB_OK;
+      };
+      for (size_t c = 0; c < nc; ++c)
+      {
+        const int b = (int)(c % depth);
+        const size_t r0 = c * chunk, nr = std::min(chunk, rows - r0);
+        // the pinned buffer's previous chunk was drained lag chunks ago
+        e = cudaMemcpy2DAsync(pinned().buf[1][b], rb, static_cast<const char *>(dev) + r0 * dp, dp, rb, nr,
+                              cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) return cuda_error(e, "device->host copy");
+        cudaEventRecord(p->ev_h[1][b], st);
+        if (c >= (size_t)lag && (rc = drain(c - lag))) return rc;
+      }
+      for (size_t c = nc > (size_t)lag ? nc - lag : 0; c < nc; ++c)
+        if ((rc = drain(c))) return rc;
+      return FCB_OK;
+    }
   }
-  const int depth = stage_depth(), lag = depth - 1;
-  const size_t chunk = std::max<size_t>(1, (size_t)stage_bytes() / rb);
-  int rc = ensure_host_staging(p, 1, std::min(chunk, rows) * rb, depth);
-  if (rc) return rc;
-  const size_t nc = (rows + chunk - 1) / chunk;
-  auto drain = [&](size_t c) -> int {
-    const int b = (int)(c % depth);
-    const size_t r0 = c * chunk, nr = std::min(chunk, rows - r0);
-    const cudaError_t e2 = cudaEventSynchronize(p->ev_h[1][b]);
-    if (e2 != cudaSuccess) return cuda_error(e2, "device->host copy");
-    host_copy_rows(static_cast<char *>(host) + r0 * hp, hp, p->hstage[1][b], rb, rb, nr);
-    return FCB_OK;
-  };
-  for (size_t c = 0; c < nc; ++c)
-  {
-    const int b = (int)(c % depth);
-    const size_t r0 = c * chunk, nr = std::min(chunk, rows - r0);
-    // the pinned buffer's previous chunk was drained lag chunks ago
-    e = cudaMemcpy2DAsync(p->hstage[1][b], rb, static_cast<const char *>(dev) + r0 * dp, dp, rb, nr,
-                          cudaMemcpyDeviceToHost, st);
-    if (e != cudaSuccess) return cuda_error(e, "device->host copy");
-    cudaEventRecord(p->ev_h[1][b], st);
-    if (c >= (size_t)lag && (rc = drain(c - lag))) return rc;
-  }
-  for (size_t c = nc > (size_t)lag ? nc - lag : 0; c < nc; ++c)
-    if ((rc = drain(c))) return rc;
-  return FCB_OK;
+  e = cudaMemcpy2DAsync(host, hp, dev, dp, rb, rows, cudaMemcpyDeviceToHost, st);
+  return e == cudaSuccess ? FCB_OK : cuda_error(e, "device->host copy");
 }
 
+// A host-buffer call returns only once none of its copies is queued or running,
+// on an error too: its caller may free or reuse the host buffers as soon as
+// the call returns.  Waits for the plan's streams and keeps the first error.
 int host_done(fcb_plan p, int rc, const char *what)
 {
   const cudaStream_t ss[3] = {p->cin, p->cout, p->stream};
@@ -713,7 +748,12 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
     const size_t in_span = sizeof(float2) * (size_t)((rows - 1) * in_rs + p->n);
     const size_t out_span = sizeof(float2) * (size_t)((rows - 1) * out_rs + p->n);
     const bool stage_in = host_pageable(in, in_span), stage_out = host_pageable(out, out_span);
-    if (stage_in || stage_out) return exec_host_staged(p, in, in_rs, out, out_rs, rows, stage_in, stage_out);
+    if (stage_in || stage_out)
+    {
+      const int rc = exec_host_staged(p, in, in_rs, out, out_rs, rows, stage_in, stage_out);
+      if (rc != kNoPinned) return rc;
+      // no pinned memory to be had: the CUDA runtime copies the pageable memory
+    }
   }
   // A queued call (sync = false) is expected to have neighbours on the link:
   // it moves twice the chunk size per copy and skips the ramps below (fewer,
@@ -801,13 +841,15 @@ int exec_host(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long l
 }
 
 // Host call with pageable input and/or output: each chunk is copied by the
-// copy threads into a pinned buffer of the plan, moved in, transformed, moved
-// out into another pinned buffer and copied to the caller's rows, while the
-// copy engines and the kernels work on the neighbouring chunks.  A pinned side
-// moves directly.  Returns when the output is written, queued or not.
+// copy threads into a shared pinned buffer, moved in, transformed, moved out
+// into another pinned buffer and copied to the caller's rows, while the copy
+// engines and the kernels work on the neighbouring chunks.  A pinned side
+// moves directly.  Returns when the output is written, queued or not;
+// kNoPinned, before any work, if the pinned buffers could not be had.
 int exec_host_staged(fcb_plan p, const float2 *in, long long in_rs, float2 *out, long long out_rs,
                      long long rows, bool stage_in, bool stage_out)
 {
+  std::lock_guard<std::mutex> lk(pinned().mu);
   const size_t row_bytes = sizeof(float2) * (size_t)p->n;
   long long chunk = std::max<long long>(1, stage_bytes() / (long long)row_bytes);
   long long alloc = 2 * chunk;  // the device buffers as the pinned path sizes them
@@ -836,7 +878,7 @@ int exec_host_staged(fcb_plan p, const float2 *in, long long in_rs, float2 *out,
     const long long r0 = d * chunk, nr = std::min(chunk, rows - r0);
     const cudaError_t e = cudaEventSynchronize(p->ev_h[1][b]);
     if (e != cudaSuccess) return cuda_error(e, "device->host copy");
-    host_copy_rows(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, p->hstage[1][b], row_bytes, row_bytes,
+    host_copy_rows(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, pinned().buf[1][b], row_bytes, row_bytes,
                    (size_t)nr);
     return FCB_OK;
   };
@@ -851,8 +893,8 @@ int exec_host_staged(fcb_plan p, const float2 *in, long long in_rs, float2 *out,
       // the pinned buffer's previous chunk has moved in
       cudaError_t e = cudaEventSynchronize(p->ev_h[0][b]);
       if (e != cudaSuccess) return host_done(p, cuda_error(e, "host->device copy"), "fcb_exec (host)");
-      host_copy_rows(p->hstage[0][b], row_bytes, src, sizeof(float2) * (size_t)in_rs, row_bytes, (size_t)nr);
-      src = p->hstage[0][b];
+      host_copy_rows(pinned().buf[0][b], row_bytes, src, sizeof(float2) * (size_t)in_rs, row_bytes, (size_t)nr);
+      src = pinned().buf[0][b];
       src_rs = p->n;
     }
     float2 *buf = p->stage[b];
@@ -870,7 +912,7 @@ int exec_host_staged(fcb_plan p, const float2 *in, long long in_rs, float2 *out,
     cudaEventRecord(p->ev_k[b], p->stream);
     cudaStreamWaitEvent(p->cout, p->ev_k[b], 0);
     // the output's pinned buffer was drained on the host depth chunks ago
-    e = stage_out ? cudaMemcpyAsync(p->hstage[1][b], buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
+    e = stage_out ? cudaMemcpyAsync(pinned().buf[1][b], buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
         : out_rs == p->n
           ? cudaMemcpyAsync(out + r0 * out_rs, buf, row_bytes * (size_t)nr, cudaMemcpyDeviceToHost, p->cout)
           : cudaMemcpy2DAsync(out + r0 * out_rs, sizeof(float2) * (size_t)out_rs, buf, row_bytes, row_bytes,

@@ -5,8 +5,8 @@
 // own, one copy at a time and synchronously with the calling thread: a
 // 128 MB in / 128 MB out call measured about 5.6 GB/s each way that way,
 // against 42-46 GB/s from pinned memory.  Host calls on pageable buffers
-// therefore copy each chunk into a pinned buffer of the plan (and out of one)
-// with several threads at once, while the copy engines move the neighbouring
+// therefore copy each chunk into a shared pinned buffer (and out of one) with
+// several threads at once, while the copy engines move the neighbouring
 // chunks.
 #include "fcb_internal.h"
 
