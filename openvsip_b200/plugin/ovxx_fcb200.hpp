@@ -59,6 +59,8 @@
 
 #include <fcb200.h>
 
+#include <algorithm>
+#include <atomic>
 #include <complex>
 #include <cstdio>
 #include <cstdlib>
@@ -67,6 +69,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace ovxx
@@ -87,6 +90,37 @@ inline void check(int rc)
   std::string msg = std::string("fcb200: ") + fcb_last_error();
   if (rc == FCB_ERR_NOMEM) OVXX_DO_THROW(std::bad_alloc());
   OVXX_DO_THROW(std::runtime_error(msg));
+}
+
+// True when the rows x cols values at a (row stride a_rs) equal those at b
+// (row stride b_rs).  Large matrices are compared in row ranges on several
+// threads: a 1024 x 16384 weight matrix is 128 MB on each side, which one
+// thread reads in about as long as the fused call takes.
+template <typename T>
+bool equal_rows(T const *a, stride_type a_rs, T const *b, stride_type b_rs, length_type rows, length_type cols)
+{
+  size_t const rb = sizeof(T) * cols;
+  unsigned nt = std::min(8u, std::max(1u, std::thread::hardware_concurrency() / 2));
+  if ((size_t)rows * rb < (size_t(8) << 20) || rows < nt) nt = 1;
+  std::atomic<bool> differ(false);
+  auto part = [&](unsigned k) {
+    length_type const r0 = rows * k / nt, r1 = rows * (k + 1) / nt;
+    for (length_type r = r0; r < r1 && !differ.load(std::memory_order_relaxed); ++r)
+      if (std::memcmp(a + r * a_rs, b + r * b_rs, rb) != 0) differ.store(true);
+  };
+  std::vector<std::thread> ts;
+  unsigned started = 1;
+  try
+  {
+    for (; started < nt; ++started) ts.emplace_back(part, started);
+  }
+  catch (...)
+  {
+  }  // no thread to be had: this one takes the remaining ranges
+  for (unsigned k = started; k < nt; ++k) part(k);
+  part(0);
+  for (auto &t : ts) t.join();
+  return !differ.load();
 }
 
 // Select the device once per thread (reference library init is per thread,
@@ -153,9 +187,8 @@ public:
   fcb_plan fused(ctype const *w, stride_type w_rs, length_type wrows, float s, length_type rows_max)
   {
     size_t const n = (size_t)(wrows * cols_);
-    bool same = fused_ && fused_rows_ == wrows && fused_scale_ == s && fused_w_.size() == n;
-    for (length_type r = 0; same && r < wrows; ++r)
-      same = std::memcmp(&fused_w_[r * cols_], w + r * w_rs, sizeof(ctype) * cols_) == 0;
+    bool const same = fused_ && fused_rows_ == wrows && fused_scale_ == s && fused_w_.size() == n &&
+                      equal_rows(fused_w_.data(), (stride_type)cols_, w, w_rs, wrows, cols_);
     if (same) return fused_;
     if (fused_) fcb_destroy(fused_);
     fused_ = 0;

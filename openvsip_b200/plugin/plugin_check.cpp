@@ -3,10 +3,12 @@
 // so that a test can compare them with the FP64 oracle.
 //
 //   plugin_check ROWS COLS in.bin weights.bin out_prefix
-// writes out_prefix.{phased,fused,fusedm}.bin: the phased Fftm -> vmmul -> Fftm
+// writes out_prefix.{phased,fused,fusedm,fusedm2,fusedm3}.bin: the phased Fftm -> vmmul -> Fftm
 // form (benchmarks/fastconv.cpp:100-106), the fused by-value expression
 // (tests/fastconv.cpp:204) and the matrix-of-coefficients expression with each
-// row's weights equal to the vector times (1 + row/ROWS); and
+// row's weights equal to the vector times (1 + row/ROWS), called twice
+// (fusedm, fusedm2: the second reuses the cached plan) and once more after
+// the last row's last weight is doubled (fusedm3); and
 // out_prefix.{fft2d,fft2d_rt}.bin: the 2-D vsip::Fft of the input and the
 // inverse 2-D Fft (scale 1 / (ROWS COLS), by value) of that result.
 #include "ovxx_fcb200.hpp"
@@ -72,6 +74,12 @@ int main(int argc, char **argv)
     save(prefix + ".fused.bin", out);
     out = inv_fftm(wm * for_fftm(in));
     save(prefix + ".fusedm.bin", out);
+    // the same weights again (the cached fused plan), then one weight changed
+    out = inv_fftm(wm * for_fftm(in));
+    save(prefix + ".fusedm2.bin", out);
+    wm.put(rows - 1, cols - 1, wm.get(rows - 1, cols - 1) * 2.f);
+    out = inv_fftm(wm * for_fftm(in));
+    save(prefix + ".fusedm3.bin", out);
   }
   {
     Fft<const_Matrix, cf, cf, fft_fwd, by_reference> f2(Domain<2>(rows, cols), 1.0);

@@ -97,7 +97,7 @@ def test_reference_fftm_regressions_on_b200(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rows,cols", [(64, 4096), (8, 32768)])
+@pytest.mark.parametrize("rows,cols", [(64, 4096), (8, 32768), (256, 4096)])
 def test_plugin_forms_match_oracle(oracle, tmp_path, rows, cols):
     rng = np.random.default_rng(rows + cols)
     x = crandn(rng, (rows, cols))
@@ -114,7 +114,14 @@ def test_plugin_forms_match_oracle(oracle, tmp_path, rows, cols):
     wm = (w[None, :] * (1 + np.arange(rows, dtype=np.float32)[:, None] / rows)).astype(np.complex64)
     ym = np.fromfile(tmp_path / "out.fusedm.bin", dtype=np.complex64).reshape(rows, cols)
     assert oracle.rel_l2(ym, oracle.fastconv(x, wm)) <= 2e-6
-    assert r.stderr.count("fused fastconv") >= 2
+    # the cached plan for unchanged weights (256 x 4096: an 8 MB weight matrix,
+    # compared on several threads), a new one after one weight changed
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "out.fusedm2.bin", dtype=np.complex64).reshape(rows, cols), ym)
+    wm[-1, -1] *= 2
+    ym3 = np.fromfile(tmp_path / "out.fusedm3.bin", dtype=np.complex64).reshape(rows, cols)
+    assert oracle.rel_l2(ym3[-1:], oracle.fastconv(x[-1:], wm[-1:])) <= 2e-6
+    np.testing.assert_array_equal(ym3[:-1], ym[:-1])
+    assert r.stderr.count("fused fastconv") >= 4
     # the 2-D vsip::Fft forward (by reference) and inverse (by value, scale 1 / (rows cols))
     y2 = np.fromfile(tmp_path / "out.fft2d.bin", dtype=np.complex64).reshape(rows, cols)
     assert oracle.rel_l2(y2, np.fft.fft2(x.astype(np.complex128))) <= 2e-6
