@@ -167,6 +167,25 @@ def cpu_reference_sample(rows_per_proc: int = 1):
             "seconds": wall}
 
 
+def plugin_sample(rows: int, cols: int, loops: int):
+    """The same workload through the reference's own vsip API with the B200
+    plugin included (openvsip_b200/plugin/_bin/plugin_bench, built where the
+    reference sources exist): vsip::Matrix blocks in pageable host memory, the
+    fused by-value expression and the phased Impl1op form, wall-clock timed."""
+    prog = os.path.join(ROOT, "openvsip_b200", "plugin", "_bin", "plugin_bench")
+    if not os.path.exists(prog):
+        return None
+    r = subprocess.run([prog, str(rows), str(cols), str(loops)], capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        return {"error": r.stderr[-300:]}
+    o = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": o["fused_samples_per_s"], "unit": "complex samples/s",
+            "phased": {"value": o["phased_samples_per_s"], "unit": "complex samples/s"}, "loops": loops,
+            "how": "reference vsip API + B200 plugin (plugin_bench): out = inv_fftm(vmmul<0>(replica, "
+                   "for_fftm(data))) by value, one fused B200 pass per call; phased: Fftm by reference, "
+                   "vmmul<0> on the host, Fftm; vsip::Matrix blocks in pageable host memory"}
+
+
 def cpu_port_sample():
     """Fallback when oracle/_ref is absent: the oracle's FP32 radix-2 port."""
     from oracle import oracle
@@ -845,6 +864,7 @@ def main():
     e2e_pg_s = time.perf_counter() - t0
     e2e_pg_value = samples_step * e2e_steps * world / shard.max_over_ranks(e2e_pg_s)
     del pout
+    plugin = plugin_sample(pulses, nsamp, min(e2e_steps, 5)) if world == 1 else None
 
     # the served stream on one GPU (first: its latencies are the most sensitive to what ran
     # before), then the uneven batch on every rank (jobs partitioned across ranks)
@@ -904,8 +924,8 @@ def main():
                                                   "for its result"},
                     "pageable": {"value": e2e_pg_value, "unit": "complex samples/s",
                                  "how": "Fastconv(numpy pageable in, numpy pageable out), each call waits for its "
-                                        "result; chunks staged through the plan's pinned buffers by host "
-                                        "threads"}},
+                                        "result; chunks staged through pinned buffers by host threads"},
+                    "plugin": plugin},
             "phased": phased,
             "matrix_of_coefficients": matrix,
             "batch": batch,
