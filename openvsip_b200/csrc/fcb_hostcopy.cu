@@ -15,15 +15,61 @@
 #include <algorithm>
 #include <atomic>
 #include <condition_variable>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <thread>
 #include <unistd.h>
+#if defined(__x86_64__)
+#include <emmintrin.h>
+#endif
 
 namespace fcb {
 
 namespace {
+
+// memcpy with non-temporal stores for the 16-byte aligned body (x86-64): the
+// destination lines are written without being read first, and stay out of
+// the caches (the copy engine or the caller reads them next, not this thread).
+// The caller fences (sfence) before another thread or a DMA reads the data.
+inline void stream_copy(char *dst, const char *src, size_t n)
+{
+#if defined(__x86_64__)
+  const size_t head = (16 - (reinterpret_cast<uintptr_t>(dst) & 15)) & 15;
+  if (n < head + 256)
+  {
+    std::memcpy(dst, src, n);
+    return;
+  }
+  std::memcpy(dst, src, head);
+  dst += head;
+  src += head;
+  n -= head;
+  const size_t body = n & ~size_t(63);
+  for (size_t i = 0; i < body; i += 64)
+  {
+    const __m128i a = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i));
+    const __m128i b = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 16));
+    const __m128i c = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 32));
+    const __m128i d = _mm_loadu_si128(reinterpret_cast<const __m128i *>(src + i + 48));
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i), a);
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 16), b);
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 32), c);
+    _mm_stream_si128(reinterpret_cast<__m128i *>(dst + i + 48), d);
+  }
+  std::memcpy(dst + body, src + body, n - body);
+#else
+  std::memcpy(dst, src, n);
+#endif
+}
+
+inline void store_fence()
+{
+#if defined(__x86_64__)
+  _mm_sfence();
+#endif
+}
 
 // One job at a time (callers serialise on job_mu_); the calling thread works
 // on its own job next to the workers.  Pieces are whole rows, or for dense
@@ -81,11 +127,11 @@ private:
     if (dense_)
     {
       const size_t b0 = k * piece_, nb = std::min(piece_, total_ - b0);
-      std::memcpy(dst_ + b0, src_ + b0, nb);
+      stream_copy(dst_ + b0, src_ + b0, nb);
       return;
     }
     const size_t r0 = k * piece_, r1 = std::min(rows_, r0 + piece_);
-    for (size_t r = r0; r < r1; ++r) std::memcpy(dst_ + r * dp_, src_ + r * sp_, rb_);
+    for (size_t r = r0; r < r1; ++r) stream_copy(dst_ + r * dp_, src_ + r * sp_, rb_);
   }
 
   // Claim pieces until none is left.  A worker counts itself active from the
@@ -99,6 +145,7 @@ private:
       piece(k);
       ++mine;
     }
+    store_fence();  // this thread's streaming stores are visible before the job counts as done
     std::lock_guard<std::mutex> lk(mu_);
     done_ += mine;
     if (worker) --active_;
