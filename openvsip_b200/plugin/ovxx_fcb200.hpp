@@ -41,7 +41,9 @@
 //
 //  3. be::user for op::fft<2, complex<float>, complex<float>, S> (the 2-D
 //     vsip::Fft<const_Matrix, ...>; backend contract src/ovxx/signal/fft/
-//     backend.hpp:294-375), through fcb_plan_fft2d.
+//     backend.hpp:294-375), through fcb_plan_fft2d, and for op::fft<1, ...>
+//     (the 1-D vsip::Fft<const_Vector, ...> that builds replica spectra;
+//     backend.hpp:132-205), through a one-row fcb_plan_fftm.
 //
 // Environment: FCB200_DEVICE selects the CUDA device (default 0);
 // FCB200_TRACE=1 prints one line per backend constructed and per fused call.
@@ -482,10 +484,83 @@ private:
   fcb_plan plan_;
 };
 
+/// fft_backend for the 1-D complex<float> FFT (vsip::Fft<const_Vector, C, C,
+/// S>, the replica's t2f in tests/fastconv.cpp:21-26 and benchmarks/
+/// fastconv.cpp:437), the contract of src/ovxx/signal/fft/backend.hpp:132-205:
+/// one row of a row plan (fcb_plan_fftm with rows_max 1), dense interleaved
+/// data (the DDA layer copies anything else), the scale applied in the kernel.
+template <int S>
+class fft1d : public signal::fft::fft_backend<1, ctype, ctype, S>
+{
+public:
+  fft1d(Domain<1> const &dom, float scale) : n_(dom.size()), plan_(0)
+  {
+    ensure_device();
+    check(fcb_plan_fftm((long long)n_, 1, S == fft_fwd ? FCB_FORWARD : FCB_INVERSE, scale, &plan_));
+    if (trace())
+      std::fprintf(stderr, "[fcb200] Fft<1,%s> %lu scale %g on the B200\n", S == fft_fwd ? "fwd" : "inv",
+                   (unsigned long)n_, (double)scale);
+  }
+  ~fft1d()
+  {
+    if (plan_) fcb_destroy(plan_);
+  }
+  virtual bool supports_scale() { return true; }
+  virtual void query_layout(Rt_layout<1> &inout)
+  {
+    inout.packing = dense;
+    inout.order = tuple<0, 1, 2>();
+    inout.storage_format = array;
+  }
+  virtual void query_layout(Rt_layout<1> &in, Rt_layout<1> &out)
+  {
+    query_layout(in);
+    out = in;
+  }
+  virtual bool requires_copy(Rt_layout<1> &) { return false; }
+  virtual void in_place(ctype *inout, stride_type stride, length_type n) { run(inout, stride, inout, stride, n); }
+  virtual void out_of_place(ctype *in, stride_type is, ctype *out, stride_type os, length_type n)
+  {
+    run(in, is, out, os, n);
+  }
+
+private:
+  void run(ctype *in, stride_type is, ctype *out, stride_type os, length_type n)
+  {
+    OVXX_PRECONDITION(is == 1 && os == 1 && n == n_);
+    check(fcb_exec(plan_, reinterpret_cast<fcb_cf32 const *>(in), (long long)n, reinterpret_cast<fcb_cf32 *>(out),
+                   (long long)n, 1, FCB_HOST));
+  }
+
+  length_type n_;
+  fcb_plan plan_;
+};
+
 } // namespace ovxx::fcb200
 
 namespace dispatcher
 {
+
+/// 1-D complex<float> Fft on the B200 (be::user slot, the first entry of
+/// List<op::fft> in src/ovxx/signal/fft.hpp:41-49); lengths the row plans do
+/// not support fall through to the next backend in the list.
+template <int S, vsip::return_mechanism_type R, unsigned N>
+struct Evaluator<op::fft<1, std::complex<float>, std::complex<float>, S, R, N>, be::user,
+                 std::unique_ptr<signal::fft::fft_backend<1, std::complex<float>, std::complex<float>, S> >
+                 (Domain<1> const &, float)>
+{
+  typedef signal::fft::fft_backend<1, std::complex<float>, std::complex<float>, S> backend_type;
+  static bool const ct_valid = true;
+  static char const *name() { return "fcb200 fft 1-D (B200)"; }
+  static bool rt_valid(Domain<1> const &dom, float)
+  {
+    return dom.size() > 0 && fcb_supported_length((long long)dom.size());
+  }
+  static std::unique_ptr<backend_type> exec(Domain<1> const &dom, float scale)
+  {
+    return std::unique_ptr<backend_type>(new fcb200::fft1d<S>(dom, scale));
+  }
+};
 
 /// 2-D complex<float> Fft on the B200 (be::user slot, the first entry of
 /// List<op::fft> in src/ovxx/signal/fft.hpp:41-49).  Any dimensions the row

@@ -44,6 +44,7 @@ def test_reference_fastconv_test_on_b200():
     assert "[fcb200] Fftm<fwd>" in r.stderr
     assert "[fcb200] fused fastconv" in r.stderr and "vector weights" in r.stderr
     assert "matrix weights" in r.stderr
+    assert "[fcb200] Fft<1,fwd>" in r.stderr  # the replica's t2f (1-D vsip::Fft)
 
 
 @pytest.mark.gpu
@@ -58,6 +59,18 @@ def test_reference_fftm_test_on_b200():
     for n in (16, 128, 242):
         assert f"[fcb200] Fftm<real->complex, col> n {n} x 5" in r.stderr
         assert f"[fcb200] Fftm<complex->real, col> n {n} x 5" in r.stderr
+
+
+@pytest.mark.gpu
+def test_reference_fft_test_on_b200():
+    # tests/fft.cpp: 1-D complex FFTs by reference and by value, interleaved and
+    # split storage, at 64, 128, 256, 512 and at 68, 252, 17 (Bluestein), each
+    # checked by the test itself; its real cases stay on the generic backend
+    r = _run([_prog("fft_test")])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for n in (64, 256, 512, 68, 252, 17):
+        assert f"[fcb200] Fft<1,fwd> {n} " in r.stderr, n
+        assert f"[fcb200] Fft<1,inv> {n} " in r.stderr, n
 
 
 @pytest.mark.gpu
@@ -94,6 +107,17 @@ def test_reference_fftm_regressions_on_b200(name):
     r = _run([_prog("reg_" + name)])
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "[fcb200] Fftm<" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["fft_inter_split", "fft_unaligned", "fft_expr_arg"])
+def test_reference_fft_regressions_on_b200(name):
+    # tests/regressions for the 1-D vsip::Fft: interleaved <-> split storage by
+    # reference, by value and of expressions (256), unaligned subviews in and
+    # out of place (256), an expression argument with a decimated subview
+    r = _run([_prog("reg_" + name)])
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    assert "[fcb200] Fft<1," in r.stderr
 
 
 @pytest.mark.gpu
