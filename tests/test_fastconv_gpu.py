@@ -154,3 +154,33 @@ def test_fastconv_accuracy_vs_fp32_cpu(oracle, case):
         y = fc(dx).cpu().numpy()
         err = oracle.rel_l2(y, want)
         assert err <= RTOL and err <= 2 * cpu_err, (err, cpu_err)
+
+
+def test_calls_follow_the_current_torch_stream(oracle):
+    # a plan binds the current torch stream only when it changes: calls made
+    # alternately under two streams, each on an input produced on its stream
+    # behind a long kernel (a call queued on another stream would read that
+    # input before it is written), must all equal the FP64 result
+    import torch
+    rng = np.random.default_rng(31)
+    rows, n = 64, 4096
+    rep = crandn(rng, (n,))
+    x = torch.from_numpy(crandn(rng, (rows, n))).cuda()
+    want = oracle.fastconv(x.cpu().numpy(), rep)
+    fc = Fastconv(rep, rows)
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = []
+    for k in range(6):
+        s = streams[k % 2]
+        with torch.cuda.stream(s):
+            torch.cuda._sleep(2_000_000)  # keeps the stream busy for about a millisecond
+            xk = x * 1  # written on s after the sleep
+            y = torch.empty_like(x)
+            fc(xk, y)
+            w = torch.empty_like(x)
+            vmmul(torch.ones(n, dtype=torch.complex64, device="cuda"), y, w)
+            outs.append((s, y, w))
+    for s, y, w in outs:
+        s.synchronize()
+        assert oracle.rel_l2(y.cpu().numpy(), want) <= 2e-6
+        np.testing.assert_array_equal(w.cpu().numpy(), y.cpu().numpy())
