@@ -303,10 +303,14 @@ static void init_table()
         // defaults (measured): 4 CTAs of 128 threads per SM for rows of 256 ..
         // 4096 samples, 256-thread CTAs for 8192, 512-thread CTAs from 16384
         // up (clusters of 2 and 4 of them for 32768 and 65536; clusters of
-        // smaller CTAs measured slower at every length), except the fused
-        // fast convolution of 16384-sample rows: the wide variant (one stage,
-        // two slot exchanges fewer), 13 % faster
-        g_variant[l][m] = (l == kWideLog && m == kFastconv) ? 3 : (l >= 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
+        // smaller CTAs measured slower at every length), except the wide
+        // variant for the fused fast convolution of 16384-sample rows (one
+        // stage, two slot exchanges fewer: 13 % faster) and for the forward and
+        // inverse transforms of 32768-sample rows (clusters of two wide CTAs:
+        // 2.8 % / 1.7 % faster; the fused form there measured the same)
+        g_variant[l][m] = (l == kWideLog && m == kFastconv) ? 3
+                        : (l == kWideMaxLog && m != kFastconv) ? 3
+                        : (l >= 14) ? 1 : (l >= kMin128 && l <= 12) ? 2 : 0;
   });
 }
 
