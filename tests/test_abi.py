@@ -84,3 +84,16 @@ def test_empty_arrays_are_described_without_strides():
     from openvsip_b200.vsip import _desc
     assert _desc(np.zeros((0, 1024), dtype=np.complex64), False)[1:] == (0, 1024, 1024, 0)
     assert _desc(np.zeros((0, 16), dtype=np.float32), False, real=True)[1:] == (0, 16, 16, 0)
+
+
+def test_python_api_rejects_unsuitable_tensors():
+    # the tensor checks run before any library call: host (CPU) tensors, other
+    # dtypes, more than two dimensions and non-unit-stride rows are refused
+    import torch
+    from openvsip_b200.vsip import _desc
+    with pytest.raises(TypeError):
+        _desc(torch.zeros(2, 4, dtype=torch.complex64), False)  # host tensor: use numpy for host data
+    with pytest.raises(TypeError):
+        _desc(torch.zeros(2, 4, dtype=torch.complex128), False)
+    with pytest.raises(TypeError):
+        _desc(torch.zeros(2, 4, dtype=torch.complex64), False, real=True)
